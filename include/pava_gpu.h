@@ -1,0 +1,149 @@
+/*
+ * pava_gpu.h -- C ABI of the pava B200 SpMV engine (sm_100a).
+ *
+ * Plain pointers, sizes and status codes only; device pointers are CUDA device addresses and
+ * a stream is passed as `void *` (a cudaStream_t, or NULL for the default stream).  Every entry
+ * point returns a pava_status (or the reference's int convention where it mirrors a
+ * reference function), never exits and never aborts.
+ *
+ * Each declaration names the reference interface it replaces (path:line in the reference
+ * tree).  The engine is CUDA throughout: there is no CPU fallback, and an entry point that
+ * needs the GPU reports PAVA_E_CUDA when none is usable.
+ */
+#ifndef PAVA_GPU_H
+#define PAVA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  0 .. -5 keep the values of the reference's ANONYMOUSLIB codes
+ * (csr5/detail/common.h:13-18); the rest are new. */
+typedef enum pava_status {
+    PAVA_SUCCESS = 0,                  /* ANONYMOUSLIB_SUCCESS */
+    PAVA_E_UNKNOWN_FORMAT = -1,        /* ANONYMOUSLIB_UNKOWN_FORMAT */
+    PAVA_E_UNSUPPORTED_PARAMS = -2,    /* ANONYMOUSLIB_UNSUPPORTED_CSR5_OMEGA: tile parameters */
+    PAVA_E_CONVERT_FAILED = -3,        /* ANONYMOUSLIB_CSR_TO_CSR5_FAILED */
+    PAVA_E_NOT_CONVERTED = -4,         /* ANONYMOUSLIB_UNSUPPORTED_CSR_SPMV: spmv before asCSR5 */
+    PAVA_E_UNSUPPORTED_VALUE_TYPE = -5,/* ANONYMOUSLIB_UNSUPPORTED_VALUE_TYPE */
+    PAVA_E_INVALID_ARG = -10,
+    PAVA_E_INVALID_CSR = -11,          /* row_ptr not monotone / column out of range */
+    PAVA_E_CUDA = -12,                 /* CUDA error or no usable GPU */
+    PAVA_E_NOMEM = -13,
+    PAVA_E_TIMEOUT = -14,              /* a bounded device wait gave up */
+    PAVA_E_TOO_LARGE = -15             /* sizes beyond the int32 element space */
+} pava_status;
+
+/* Storage formats.  CSR and CSR5 keep the reference's ANONYMOUSLIB_FORMAT_* values
+ * (csr5/detail/common.h:20-22); CVR is cvr/cvr.h's format. */
+typedef enum pava_format {
+    PAVA_FORMAT_CSR = 0,   /* plain CSR, lanes-per-row vector kernel (baseline and checker) */
+    PAVA_FORMAT_CSR5 = 1,  /* CSR5 tiles: 32 lanes x sigma, bit-flag descriptors */
+    PAVA_FORMAT_CVR = 3    /* CVR chunks: 32 lanes x S steps, row-completion bits */
+} pava_format;
+
+typedef enum pava_precision {
+    PAVA_PREC_FP64 = 0,    /* values, x, y FP64; FMA accumulation */
+    PAVA_PREC_FP32C = 1    /* values and x FP32, compensated FP32 accumulation, FP64 carries
+                              and FP64 y */
+} pava_precision;
+
+typedef enum pava_index_mode {
+    PAVA_INDEX_I32 = 0,    /* 32-bit column indices */
+    PAVA_INDEX_DELTA16 = 1 /* 16-bit column offsets from the row index (|col - row| < 32768) */
+} pava_index_mode;
+
+/* A CSR matrix, 0-based, sorted or unsorted columns, FP64 values (the reference's
+ * _PAVA_CSRMatrix, utils/basicMatrix.h:51-60). */
+typedef struct pava_csr {
+    int m, n, nnz;
+    const int *row_ptr;   /* m + 1 */
+    const int *col_idx;   /* nnz   */
+    const double *vals;   /* nnz   */
+    int on_device;        /* 1: the three arrays are device memory; 0: host memory */
+} pava_csr;
+
+/* Tuning knobs; zero means "default". */
+typedef struct pava_opts {
+    int steps;            /* CVR: steps per warp chunk, a multiple of 32 (default 64) */
+    int sigma;            /* CSR5: elements per lane per tile, multiple of 4, <= 32 (default 16) */
+    int tiles_per_chunk;  /* CSR5: tiles per warp chunk (default 4) */
+    int precision;        /* pava_precision */
+    int index_mode;       /* pava_index_mode */
+    int lanes_per_row;    /* CSR: 1, 2, 4, 8, 16 or 32 (default: from the mean row length) */
+} pava_opts;
+
+typedef struct pava_info {
+    int format, precision, index_mode;
+    int m, n, nnz, n_empty;
+    long long chunks;          /* warp chunks (CVR, CSR5) or rows (CSR) */
+    long long elems_per_chunk;
+    double convert_ms;         /* device time of the conversion */
+    size_t device_bytes;       /* bytes the handle holds on the device */
+    double alg_bytes;          /* compulsory bytes of one SpMV: nnz*(s_v+s_i) + 4(m+1) + n*s_x
+                                  + m*s_y (x and y counted once) */
+    double format_bytes;       /* bytes one SpMV streams from the format (values, columns,
+                                  flags, metadata) plus x and y */
+} pava_info;
+
+typedef struct pava_handle pava_handle;
+
+/* Selects the CUDA device for the calling thread (cudaSetDevice). */
+pava_status pava_init(int device);
+
+/* Converts A into `format` on the device (the GPU form of anonymouslibHandle::inputCSR +
+ * asCSR5, csr5/anonymouslib_avx512.h:58-70,107-221, and of CVR's pre_processing,
+ * cvr/cvr.h:583-1060).  The caller's arrays are never modified (the reference transposes
+ * them in place, format_avx512.h:428).  The conversion is validated first: a row_ptr that
+ * is not monotone or a column outside [0, n) gives PAVA_E_INVALID_CSR. */
+pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, void *stream,
+                        pava_handle **out);
+
+/* y = A x on the device (anonymouslibHandle::spmv, csr5/anonymouslib_avx512.h:234-256;
+ * spmv_compute_kernel, cvr/cvr.h:1062).  FP64 handles take double x and write double y;
+ * FP32C handles take float x and write double y.  Every call overwrites all m entries of y
+ * (empty rows become 0), so repeated calls give identical results -- unlike the reference,
+ * whose repeated calls accumulate into shared rows (cvr/cvr.h:1415; csr5_spmv_avx512.h:277). */
+pava_status pava_spmv(pava_handle *h, const void *x, void *y, void *stream);
+
+/* pava_spmv split into its launches, for timing one kernel: stage 1 runs the format's SpMV
+ * kernel, stage 2 the carry fixup that finishes rows shared between warp chunks (CVR and
+ * CSR5; a no-op for CSR), stage 0 both (= pava_spmv).  y is complete only after stage 2.
+ * No counterpart in the reference. */
+pava_status pava_spmv_stage(pava_handle *h, const void *x, void *y, void *stream, int stage);
+
+/* End-to-end form of pava_spmv on host buffers: copies x host->device, runs the SpMV and
+ * copies y device->host on `stream`, then synchronises it.  Buffers for x and y are kept on
+ * the handle after the first call. */
+pava_status pava_spmv_host(pava_handle *h, const void *x_host, void *y_host, void *stream);
+
+pava_status pava_get_info(const pava_handle *h, pava_info *out);
+
+/* anonymouslibHandle::destroy / asCSR (csr5/anonymouslib_avx512.h:80-104,258-262). */
+pava_status pava_destroy(pava_handle *h);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *pava_last_error(void);
+const char *pava_status_string(int status);
+
+/* Drop-ins for the reference's engine entry points, same signatures and meaning:
+ * conduct_cvr (cvr/cvr.h:1953) and conduct_csr5 (csr5/csr5.h:72-74).  Each copies the CSR to
+ * the device, converts (timed as the convert column), runs one SpMV into refOut / y (the
+ * checked result), times numIterations more, and prints the reference's line
+ * " Performance <name> CVR|CSR5 <SMs> <convert s> <exec s>" (utils/basicMatrix.cpp:491-495).
+ * Returns 0 on success or a pava_status.  alpha is accepted and, as in the reference, not
+ * applied (cvr/cvr.h never reads it; csr5_spmv_avx512.h comments out its multiply). */
+int conduct_cvr_gpu(int numRows, int numCols, int nItems_raw, int *h_rowDelimiters,
+                    int *h_cols, double *h_val, double *h_vec, double *refOut, int alpha,
+                    char *matrixName, int numIterations);
+int conduct_csr5_gpu(int m, int n, int nnzA, int *csrRowPtrA, int *csrColIdxA,
+                     double *csrValA, double *x, double *y, double alpha, char *matrixName,
+                     int numIterations);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PAVA_GPU_H */

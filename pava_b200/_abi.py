@@ -1,0 +1,148 @@
+"""ctypes bindings of the engine's C ABI (include/pava_gpu.h, include/pava_host.h).
+
+The CUDA library is the product path: if ``lib/libpava_gpu.so`` is missing, importing the
+GPU entry points raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(HERE, "lib")
+
+_GPU = None
+_HOST = None
+
+c_int, c_ll, c_dbl, c_void_p, c_char_p = (ctypes.c_int, ctypes.c_longlong, ctypes.c_double,
+                                          ctypes.c_void_p, ctypes.c_char_p)
+c_u64 = ctypes.c_uint64
+c_size_t = ctypes.c_size_t
+
+# status codes (include/pava_gpu.h)
+SUCCESS = 0
+E_UNKNOWN_FORMAT = -1
+E_UNSUPPORTED_PARAMS = -2
+E_CONVERT_FAILED = -3
+E_NOT_CONVERTED = -4
+E_UNSUPPORTED_VALUE_TYPE = -5
+E_INVALID_ARG = -10
+E_INVALID_CSR = -11
+E_CUDA = -12
+E_NOMEM = -13
+E_TIMEOUT = -14
+E_TOO_LARGE = -15
+
+FORMAT_CSR, FORMAT_CSR5, FORMAT_CVR = 0, 1, 3
+PREC_FP64, PREC_FP32C = 0, 1
+INDEX_I32, INDEX_DELTA16 = 0, 1
+
+
+class PavaCsr(ctypes.Structure):
+    _fields_ = [("m", c_int), ("n", c_int), ("nnz", c_int), ("row_ptr", c_void_p),
+                ("col_idx", c_void_p), ("vals", c_void_p), ("on_device", c_int)]
+
+
+class PavaOpts(ctypes.Structure):
+    _fields_ = [("steps", c_int), ("sigma", c_int), ("tiles_per_chunk", c_int),
+                ("precision", c_int), ("index_mode", c_int), ("lanes_per_row", c_int)]
+
+
+class PavaInfo(ctypes.Structure):
+    _fields_ = [("format", c_int), ("precision", c_int), ("index_mode", c_int), ("m", c_int),
+                ("n", c_int), ("nnz", c_int), ("n_empty", c_int), ("chunks", c_ll),
+                ("elems_per_chunk", c_ll), ("convert_ms", c_dbl), ("device_bytes", c_size_t),
+                ("alg_bytes", c_dbl), ("format_bytes", c_dbl)]
+
+
+class PavaError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"pava status {status}: {msg}")
+        self.status = status
+
+
+# exported symbols and their prototypes: (name, restype, argtypes)
+GPU_SYMBOLS = [
+    ("pava_init", c_int, [c_int]),
+    ("pava_create", c_int, [ctypes.POINTER(PavaCsr), c_int, ctypes.POINTER(PavaOpts), c_void_p,
+                            ctypes.POINTER(c_void_p)]),
+    ("pava_spmv", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("pava_spmv_stage", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
+    ("pava_spmv_host", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("pava_get_info", c_int, [c_void_p, ctypes.POINTER(PavaInfo)]),
+    ("pava_destroy", c_int, [c_void_p]),
+    ("pava_last_error", c_char_p, []),
+    ("pava_status_string", c_char_p, [c_int]),
+    ("conduct_cvr_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                c_void_p, c_int, c_char_p, c_int]),
+    ("conduct_csr5_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_void_p, c_dbl, c_char_p, c_int]),
+]
+
+HOST_SYMBOLS = [
+    ("pava_gen_laplace2d_rowptr", c_int, [c_int, c_void_p]),
+    ("pava_gen_laplace2d_fill", c_int, [c_int, c_void_p, c_void_p, c_void_p]),
+    ("pava_gen_powerlaw_rowptr", c_int, [c_int, c_int, c_dbl, c_dbl, c_int, c_dbl, c_u64,
+                                         c_void_p]),
+    ("pava_gen_powerlaw_fill", c_int, [c_int, c_int, c_u64, c_void_p, c_void_p, c_void_p]),
+    ("pava_gen_stencil27_rowptr", c_int, [c_int, c_void_p]),
+    ("pava_gen_stencil27_fill", c_int, [c_int, c_u64, c_void_p, c_void_p, c_void_p]),
+    ("pava_gen_banded_rowptr", c_int, [c_int, c_int, c_int, c_void_p]),
+    ("pava_gen_banded_fill", c_int, [c_int, c_int, c_u64, c_void_p, c_void_p, c_void_p]),
+    ("pava_gen_random_rowptr", c_int, [c_int, c_int, c_dbl, c_u64, c_void_p]),
+    ("pava_gen_random_fill", c_int, [c_int, c_int, c_u64, c_void_p, c_void_p, c_void_p]),
+    ("pava_gen_blockdiag_rowptr", c_int, [c_int, c_int, c_int, c_u64, c_void_p]),
+    ("pava_gen_blockdiag_fill", c_int, [c_int, c_u64, c_void_p, c_void_p, c_void_p]),
+    ("pava_gen_uniform", c_int, [c_int, c_dbl, c_dbl, c_u64, c_int, c_void_p]),
+    ("pava_init_vectors", None, [c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    ("pava_mtx_info", c_int, [c_char_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                              ctypes.POINTER(c_ll), ctypes.POINTER(c_int),
+                              ctypes.POINTER(c_int)]),
+    ("pava_mtx_read", c_int, [c_char_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_ll)]),
+    ("pava_mtx_write", c_int, [c_char_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    ("pava_coo_to_csr", c_int, [c_int, c_int, c_ll, c_void_p, c_void_p, c_void_p, c_void_p,
+                                c_void_p, c_void_p]),
+]
+
+
+def _bind(lib, symbols):
+    for name, res, args in symbols:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def gpu_lib_path() -> str:
+    return os.path.join(LIBDIR, "libpava_gpu.so")
+
+
+def host_lib_path() -> str:
+    return os.path.join(LIBDIR, "libpava_host.so")
+
+
+def gpu():
+    """The CUDA engine.  Raises if the library is not built (no CPU fallback exists)."""
+    global _GPU
+    if _GPU is None:
+        path = gpu_lib_path()
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing: build it with `python -m pava_b200.build`")
+        _GPU = _bind(ctypes.CDLL(path), GPU_SYMBOLS)
+    return _GPU
+
+
+def host():
+    global _HOST
+    if _HOST is None:
+        path = host_lib_path()
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing: build it with `python -m pava_b200.build`")
+        _HOST = _bind(ctypes.CDLL(path), HOST_SYMBOLS)
+    return _HOST
+
+
+def check(status: int) -> None:
+    if status != SUCCESS:
+        msg = gpu().pava_last_error().decode(errors="replace")
+        raise PavaError(status, msg or gpu().pava_status_string(status).decode())

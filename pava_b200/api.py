@@ -1,0 +1,225 @@
+"""Python mirror of the reference's engine interface, backed by the CUDA engine.
+
+* ``SpMatrix``             -- a converted matrix on the GPU (pava_create / pava_spmv)
+* ``AnonymousLibHandle``   -- the CSR5 handle of csr5/anonymouslib_avx512.h:14-276 (inputCSR,
+  setX, setSigma, asCSR5, spmv, asCSR, destroy), same names, argument meaning and status codes
+* ``conduct_cvr`` / ``conduct_csr5`` -- the engine entry points of cvr/cvr.h:1953 and
+  csr5/csr5.h:72, same arguments; they print the reference's ``Performance`` line
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from .matrices import CSR
+
+FORMATS = {"csr": _abi.FORMAT_CSR, "csr5": _abi.FORMAT_CSR5, "cvr": _abi.FORMAT_CVR}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        torch = _torch()
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+class SpMatrix:
+    """A CSR matrix converted on the GPU into ``format`` ('cvr', 'csr5' or 'csr').
+
+    ``spmv(x)`` takes a CUDA tensor (float64 for FP64 handles) and returns y (float64).
+    ``spmv_host(x)`` is the end-to-end form on host arrays.
+    """
+
+    def __init__(self, A: CSR, format: str = "cvr", steps: int = 0, sigma: int = 0,
+                 tiles_per_chunk: int = 0, precision: int = _abi.PREC_FP64,
+                 index_mode: int = _abi.INDEX_I32, lanes_per_row: int = 0, stream=None,
+                 device_arrays=None):
+        L = _abi.gpu()
+        self.m, self.n, self.nnz = A.m, A.n, A.nnz
+        self.format = format
+        self.precision = precision
+        csr = _abi.PavaCsr()
+        csr.m, csr.n, csr.nnz = A.m, A.n, A.nnz
+        if device_arrays is not None:  # (rp, ci, v) CUDA tensors
+            rp, ci, v = device_arrays
+            csr.row_ptr, csr.col_idx, csr.vals = rp.data_ptr(), ci.data_ptr(), v.data_ptr()
+            csr.on_device = 1
+        else:
+            self._keep = (np.ascontiguousarray(A.rp, np.int32), np.ascontiguousarray(A.ci, np.int32),
+                          np.ascontiguousarray(A.v, np.float64))
+            csr.row_ptr = self._keep[0].ctypes.data
+            csr.col_idx = self._keep[1].ctypes.data
+            csr.vals = self._keep[2].ctypes.data
+            csr.on_device = 0
+        opts = _abi.PavaOpts(steps, sigma, tiles_per_chunk, precision, index_mode, lanes_per_row)
+        h = _abi.c_void_p()
+        _abi.check(L.pava_create(ctypes.byref(csr), FORMATS[format], ctypes.byref(opts),
+                                 _abi.c_void_p(_stream_ptr(stream) if stream is not None else None),
+                                 ctypes.byref(h)))
+        self._h = h
+        self._keep = None
+
+    # -- info ---------------------------------------------------------------------------
+    def info(self) -> dict:
+        inf = _abi.PavaInfo()
+        _abi.check(_abi.gpu().pava_get_info(self._h, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in _abi.PavaInfo._fields_}
+
+    # -- SpMV ---------------------------------------------------------------------------
+    def spmv(self, x, y=None, stream=None):
+        torch = _torch()
+        if y is None:
+            y = torch.empty(self.m, dtype=torch.float64, device=x.device)
+        want = torch.float32 if self.precision == _abi.PREC_FP32C else torch.float64
+        if x.dtype != want or not x.is_cuda or not x.is_contiguous():
+            raise TypeError(f"x must be a contiguous CUDA {want} tensor")
+        if y.dtype != torch.float64 or not y.is_cuda or y.numel() < self.m:
+            raise TypeError("y must be a CUDA float64 tensor of m entries")
+        _abi.check(_abi.gpu().pava_spmv(self._h, x.data_ptr(), y.data_ptr(),
+                                        _abi.c_void_p(_stream_ptr(stream))))
+        return y
+
+    def spmv_raw(self, x_ptr: int, y_ptr: int, stream_ptr: int | None, stage: int = 0) -> None:
+        """pava_spmv_stage on raw device pointers: stage 1 = SpMV kernel, 2 = carry fixup,
+        0 = both."""
+        _abi.check(_abi.gpu().pava_spmv_stage(self._h, x_ptr, y_ptr, _abi.c_void_p(stream_ptr),
+                                              stage))
+
+    def spmv_host(self, x, y=None, stream=None):
+        """End-to-end: host x -> device -> SpMV -> host y (numpy arrays or pinned tensors)."""
+        xa = x
+        if isinstance(x, np.ndarray):
+            want = np.float32 if self.precision == _abi.PREC_FP32C else np.float64
+            xa = np.ascontiguousarray(x, want)
+            xp = xa.ctypes.data
+        else:
+            xp = x.data_ptr()
+        if y is None:
+            y = np.empty(self.m, np.float64)
+        yp = y.ctypes.data if isinstance(y, np.ndarray) else y.data_ptr()
+        sp = _stream_ptr(stream) if stream is not None else None
+        _abi.check(_abi.gpu().pava_spmv_host(self._h, xp, yp, _abi.c_void_p(sp)))
+        return y
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _abi.gpu().pava_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- the reference's CSR5 handle ----------------------------------------------------------
+
+ANONYMOUSLIB_SUCCESS = 0
+ANONYMOUSLIB_UNKOWN_FORMAT = -1
+ANONYMOUSLIB_UNSUPPORTED_CSR5_OMEGA = -2
+ANONYMOUSLIB_CSR_TO_CSR5_FAILED = -3
+ANONYMOUSLIB_UNSUPPORTED_CSR_SPMV = -4
+ANONYMOUSLIB_UNSUPPORTED_VALUE_TYPE = -5
+ANONYMOUSLIB_FORMAT_CSR = 0
+ANONYMOUSLIB_FORMAT_CSR5 = 1
+
+
+class AnonymousLibHandle:
+    """anonymouslibHandle<int, unsigned, double> (csr5/anonymouslib_avx512.h:14-276) on the
+    GPU.  Unlike the reference, asCSR5 leaves the caller's arrays untouched and spmv writes
+    every row of y (no accumulation across calls)."""
+
+    def __init__(self, m: int, n: int):
+        self._m, self._n = int(m), int(n)
+        self._format = ANONYMOUSLIB_FORMAT_CSR
+        self._csr = None
+        self._x = None
+        self._sigma = 16
+        self._mat = None
+
+    def warmup(self) -> int:
+        return ANONYMOUSLIB_SUCCESS
+
+    def inputCSR(self, nnz, csr_row_pointer, csr_column_index, csr_value) -> int:
+        self._csr = CSR(self._m, self._n, np.ascontiguousarray(csr_row_pointer, np.int32),
+                        np.ascontiguousarray(csr_column_index, np.int32)[:nnz],
+                        np.ascontiguousarray(csr_value, np.float64)[:nnz])
+        self._format = ANONYMOUSLIB_FORMAT_CSR
+        return ANONYMOUSLIB_SUCCESS
+
+    def setX(self, x) -> int:
+        self._x = np.ascontiguousarray(x, np.float64)
+        return ANONYMOUSLIB_SUCCESS
+
+    def setSigma(self, sigma: int) -> None:
+        self._sigma = int(sigma)
+
+    def asCSR5(self) -> int:
+        if self._format == ANONYMOUSLIB_FORMAT_CSR5:
+            return ANONYMOUSLIB_SUCCESS
+        try:
+            self._mat = SpMatrix(self._csr, "csr5", sigma=self._sigma)
+        except _abi.PavaError as e:
+            if e.status == _abi.E_UNSUPPORTED_PARAMS:
+                return ANONYMOUSLIB_UNSUPPORTED_CSR5_OMEGA
+            return ANONYMOUSLIB_CSR_TO_CSR5_FAILED
+        self._format = ANONYMOUSLIB_FORMAT_CSR5
+        return ANONYMOUSLIB_SUCCESS
+
+    def spmv(self, alpha: float, y) -> int:
+        if self._format == ANONYMOUSLIB_FORMAT_CSR:
+            return ANONYMOUSLIB_UNSUPPORTED_CSR_SPMV
+        out = self._mat.spmv_host(self._x)
+        y[: self._m] = out  # alpha is not applied, as in csr5_spmv_avx512.h:334
+        return ANONYMOUSLIB_SUCCESS
+
+    def asCSR(self) -> int:
+        if self._mat is not None:
+            self._mat.close()
+            self._mat = None
+        self._format = ANONYMOUSLIB_FORMAT_CSR
+        return ANONYMOUSLIB_SUCCESS
+
+    def destroy(self) -> int:
+        return self.asCSR()
+
+
+# ---- engine entry points ------------------------------------------------------------------
+
+def _ptr(a):
+    return a.ctypes.data
+
+
+def conduct_cvr(numRows, numCols, nItems_raw, h_rowDelimiters, h_cols, h_val, h_vec, refOut,
+                alpha, matrixName, numIterations) -> int:
+    """conduct_cvr (cvr/cvr.h:1953): convert, one checked SpMV into refOut, numIterations
+    timed SpMVs, print the Performance line.  Arrays are numpy; refOut is written in place."""
+    rp = np.ascontiguousarray(h_rowDelimiters, np.int32)
+    ci = np.ascontiguousarray(h_cols, np.int32)
+    v = np.ascontiguousarray(h_val, np.float64)
+    x = np.ascontiguousarray(h_vec, np.float64)
+    assert refOut.dtype == np.float64 and refOut.flags.c_contiguous
+    return _abi.gpu().conduct_cvr_gpu(numRows, numCols, nItems_raw, _ptr(rp), _ptr(ci), _ptr(v),
+                                      _ptr(x), _ptr(refOut), int(alpha),
+                                      str(matrixName).encode(), numIterations)
+
+
+def conduct_csr5(m, n, nnzA, csrRowPtrA, csrColIdxA, csrValA, x, y, alpha, matrixName,
+                 numIterations) -> int:
+    """conduct_csr5 (csr5/csr5.h:72): same contract as conduct_cvr, CSR5 format."""
+    rp = np.ascontiguousarray(csrRowPtrA, np.int32)
+    ci = np.ascontiguousarray(csrColIdxA, np.int32)
+    v = np.ascontiguousarray(csrValA, np.float64)
+    xx = np.ascontiguousarray(x, np.float64)
+    assert y.dtype == np.float64 and y.flags.c_contiguous
+    return _abi.gpu().conduct_csr5_gpu(m, n, nnzA, _ptr(rp), _ptr(ci), _ptr(v), _ptr(xx),
+                                       _ptr(y), float(alpha), str(matrixName).encode(),
+                                       numIterations)

@@ -1,0 +1,83 @@
+"""Builds the engine's shared libraries in-tree for sm_100a.
+
+    python -m pava_b200.build
+
+* ``pava_b200/lib/libpava_gpu.so``  -- the CUDA engine and its C ABI (include/pava_gpu.h)
+* ``pava_b200/lib/libpava_host.so`` -- host-side C++: seeded matrix generators, the Matrix
+  Market reader/writer and the COO->CSR conversion (include/pava_host.h)
+
+nvcc cross-compiles for sm_100a without a GPU, so this runs on any machine with the CUDA
+toolkit.  CUDA runtime is linked statically, so the library does not depend on the
+toolkit's shared runtime at load time.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "lib")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+GPU_SOURCES = ["api.cu", "k_support.cu", "k_cvr.cu", "k_csr5.cu"]
+HOST_SOURCES = ["host/gen.cpp", "host/mtx.cpp"]
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def _stale(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def build_gpu(force: bool = False, verbose_ptxas: bool = False) -> str:
+    os.makedirs(LIBDIR, exist_ok=True)
+    out = os.path.join(LIBDIR, "libpava_gpu.so")
+    srcs = [os.path.join(CSRC, s) for s in GPU_SOURCES]
+    deps = srcs + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
+    deps.append(os.path.join(ROOT, "include", "pava_gpu.h"))
+    if not force and not _stale(out, deps):
+        return out
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    for s in srcs:
+        o = os.path.join(objdir, os.path.basename(s) + ".o")
+        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+               "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-c", s, "-o", o]
+        if verbose_ptxas:
+            cmd.insert(1, "-Xptxas=-v")
+        _run(cmd)
+        objs.append(o)
+    _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", out, *objs])
+    return out
+
+
+def build_host(force: bool = False) -> str:
+    os.makedirs(LIBDIR, exist_ok=True)
+    out = os.path.join(LIBDIR, "libpava_host.so")
+    srcs = [os.path.join(CSRC, s) for s in HOST_SOURCES]
+    deps = srcs + [os.path.join(ROOT, "include", "pava_host.h")]
+    if not force and not _stale(out, deps):
+        return out
+    _run(["g++", "-O2", "-fPIC", "-fopenmp", "-std=c++17", "-shared", "-I",
+          os.path.join(ROOT, "include"), "-o", out, *srcs])
+    return out
+
+
+def build(force: bool = False) -> None:
+    build_host(force)
+    build_gpu(force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

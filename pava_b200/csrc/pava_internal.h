@@ -1,0 +1,76 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/pava_gpu.h"
+#include "pava_common.cuh"
+
+namespace pava {
+
+// Per-chunk metadata of the GPU CVR form (128 bytes; one chunk = 32 lanes x S steps).
+// The row phase needs only the header; the rest describes the chunk's tail, where the rows
+// still open when the chunk ran out of rows are spread evenly over the 32 lanes.
+struct CvrMeta {
+    ChunkHdr h;
+    int i_t;       // first tail step (== S when the chunk has no tail)
+    int ntail;     // tail slots (rows still open at i_t, in row order), <= 64
+    int n_inprog;  // slots [0, n_inprog) hold rows a lane was working on at i_t
+    int next_g;    // slot n_inprog + j holds row r_first + next_g + j
+    unsigned cont; // bit k: lane k's first tail element continues lane k-1's last row
+    unsigned pad[3];
+    unsigned char park[32];        // slot of lane k's row in progress at i_t, 0xff if none
+    unsigned char first_slot[32];  // slot of lane k's first tail element
+    unsigned pad2[4];
+};
+static_assert(sizeof(CvrMeta) == 128, "CvrMeta layout");
+
+// Engine handle (behind the opaque pava_handle of the C ABI).
+struct Handle {
+    int format = 0, precision = 0, index_mode = 0;
+    int m = 0, n = 0, nnz = 0, n_empty = 0;
+    long long n_aug = 0;     // elements after giving every empty row one zero element
+    long long nchunks = 0;   // warp chunks
+    long long L = 0;         // elements per chunk (padded space = nchunks * L)
+    int S = 0;               // CVR: steps per chunk
+    int sigma = 0, G = 0;    // CSR5: elements per lane per tile, tiles per chunk
+    long long ntiles = 0;
+    int lanes_per_row = 0;   // plain CSR
+    int device = 0, sm_count = 0;
+
+    int *arp = nullptr;            // augmented row pointer, m + 2 entries (row m = padding)
+    void *vals = nullptr;          // format value stream
+    void *cols = nullptr;          // format column stream
+    unsigned *flags = nullptr;     // CVR row-end bits / CSR5 row-start descriptors
+    void *meta = nullptr;          // per-chunk metadata (CvrMeta or ChunkHdr)
+    size_t meta_stride = 0;
+    int *tile_ptr = nullptr;       // CSR5 tile -> first row
+    double *carry_head = nullptr;  // per-chunk partial of a first row shared with the left
+    double *carry_tail = nullptr;  // per-chunk partial of a last row shared with the right
+    int *rp = nullptr, *ci = nullptr;  // plain CSR form
+    double *v = nullptr;
+
+    double convert_ms = 0.0;
+    size_t device_bytes = 0;
+};
+
+// Kernel launchers (stream-ordered; return cudaGetLastError()).
+cudaError_t launch_validate(const int *rp, const int *ci, int m, int n, int nnz, int *d_err,
+                            cudaStream_t s);
+cudaError_t build_augmented_rowptr(const int *rp, int m, long long padded_total, int *arp,
+                                   int *d_nempty, cudaStream_t s);
+
+cudaError_t cvr_convert(Handle &h, const int *rp, const int *ci, const double *v,
+                        cudaStream_t s);
+cudaError_t cvr_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
+
+cudaError_t csr5_convert(Handle &h, const int *rp, const int *ci, const double *v,
+                         cudaStream_t s);
+cudaError_t csr5_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
+
+cudaError_t carry_fixup(const Handle &h, void *y, cudaStream_t s);
+
+cudaError_t csr_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
+
+}  // namespace pava
