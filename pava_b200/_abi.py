@@ -114,7 +114,9 @@ def _bind(lib, symbols):
 
 
 def gpu_lib_path() -> str:
-    return os.path.join(LIBDIR, "libpava_gpu.so")
+    """The engine library; PAVA_GPU_LIB names an alternative build (e.g. one compiled with
+    other launch bounds for a tuning sweep)."""
+    return os.environ.get("PAVA_GPU_LIB") or os.path.join(LIBDIR, "libpava_gpu.so")
 
 
 def host_lib_path() -> str:

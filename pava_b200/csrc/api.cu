@@ -101,36 +101,43 @@ pava_status plan_chunks(pava::Handle &h, const int *rp, cudaStream_t s) {
 pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double *v,
                     cudaStream_t s) {
     const size_t sv = value_bytes(h.precision);
-    if (h.format == PAVA_FORMAT_CVR) {
+    const size_t si = h.index_mode == PAVA_INDEX_DELTA16 ? 2 : 4;
+    if (h.format == PAVA_FORMAT_CVR || h.format == PAVA_FORMAT_CSR5) {
         pava_status st = plan_chunks(h, rp, s);
         if (st != PAVA_SUCCESS) return st;
         const size_t padded = (size_t)(h.nchunks * h.L);
         PAVA_CUDA(cudaMalloc(&h.vals, sv * (padded ? padded : 1)), "cudaMalloc(vals)");
         h.device_bytes += sv * padded;
-        PAVA_CUDA(dalloc((int **)&h.cols, padded, &h.device_bytes), "cudaMalloc(cols)");
-        PAVA_CUDA(dalloc(&h.flags, (size_t)h.nchunks * h.S, &h.device_bytes), "cudaMalloc(flags)");
-        h.meta_stride = sizeof(pava::CvrMeta);
-        PAVA_CUDA(dalloc((pava::CvrMeta **)&h.meta, (size_t)h.nchunks, &h.device_bytes),
-                  "cudaMalloc(meta)");
+        PAVA_CUDA(cudaMalloc(&h.cols, si * (padded ? padded : 1)), "cudaMalloc(cols)");
+        h.device_bytes += si * padded;
         PAVA_CUDA(dalloc(&h.carry_head, (size_t)h.nchunks, &h.device_bytes), "cudaMalloc(carry)");
         PAVA_CUDA(dalloc(&h.carry_tail, (size_t)h.nchunks, &h.device_bytes), "cudaMalloc(carry)");
-        PAVA_CUDA(pava::cvr_convert(h, rp, ci, v, s), "CVR conversion");
-    } else if (h.format == PAVA_FORMAT_CSR5) {
-        pava_status st = plan_chunks(h, rp, s);
-        if (st != PAVA_SUCCESS) return st;
-        h.ntiles = h.nchunks * h.G;
-        const size_t padded = (size_t)(h.nchunks * h.L);
-        PAVA_CUDA(cudaMalloc(&h.vals, sv * (padded ? padded : 1)), "cudaMalloc(vals)");
-        h.device_bytes += sv * padded;
-        PAVA_CUDA(dalloc((int **)&h.cols, padded, &h.device_bytes), "cudaMalloc(cols)");
-        PAVA_CUDA(dalloc(&h.flags, (size_t)h.ntiles * 32, &h.device_bytes), "cudaMalloc(desc)");
-        PAVA_CUDA(dalloc(&h.tile_ptr, (size_t)h.ntiles, &h.device_bytes), "cudaMalloc(tile_ptr)");
-        h.meta_stride = sizeof(pava::ChunkHdr);
-        PAVA_CUDA(dalloc((pava::ChunkHdr **)&h.meta, (size_t)h.nchunks, &h.device_bytes),
-                  "cudaMalloc(meta)");
-        PAVA_CUDA(dalloc(&h.carry_head, (size_t)h.nchunks, &h.device_bytes), "cudaMalloc(carry)");
-        PAVA_CUDA(dalloc(&h.carry_tail, (size_t)h.nchunks, &h.device_bytes), "cudaMalloc(carry)");
-        PAVA_CUDA(pava::csr5_convert(h, rp, ci, v, s), "CSR5 conversion");
+        int *d_ovf = nullptr;
+        PAVA_CUDA(cudaMallocAsync(&d_ovf, sizeof(int), s), "cudaMallocAsync");
+        cudaError_t e = cudaMemsetAsync(d_ovf, 0, sizeof(int), s);
+        if (h.format == PAVA_FORMAT_CVR) {
+            if (e == cudaSuccess) e = dalloc(&h.flags, (size_t)h.nchunks * h.S, &h.device_bytes);
+            h.meta_stride = sizeof(pava::CvrMeta);
+            if (e == cudaSuccess)
+                e = dalloc((pava::CvrMeta **)&h.meta, (size_t)h.nchunks, &h.device_bytes);
+            if (e == cudaSuccess) e = pava::cvr_convert(h, rp, ci, v, d_ovf, s);
+        } else {
+            h.ntiles = h.nchunks * h.G;
+            if (e == cudaSuccess) e = dalloc(&h.flags, (size_t)h.ntiles * 32, &h.device_bytes);
+            if (e == cudaSuccess) e = dalloc(&h.tile_ptr, (size_t)h.ntiles, &h.device_bytes);
+            h.meta_stride = sizeof(pava::ChunkHdr);
+            if (e == cudaSuccess)
+                e = dalloc((pava::ChunkHdr **)&h.meta, (size_t)h.nchunks, &h.device_bytes);
+            if (e == cudaSuccess) e = pava::csr5_convert(h, rp, ci, v, d_ovf, s);
+        }
+        int ovf = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&ovf, d_ovf, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaFreeAsync(d_ovf, s);
+        if (e != cudaSuccess) return fail_cuda(e, "conversion");
+        if (ovf)
+            return fail(PAVA_E_UNSUPPORTED_PARAMS,
+                        "16-bit column offsets: a column lies more than 32767 from its chunk's first row");
     } else {  // plain CSR: private copies
         PAVA_CUDA(dalloc(&h.rp, (size_t)h.m + 1, &h.device_bytes), "cudaMalloc(rp)");
         PAVA_CUDA(dalloc(&h.ci, (size_t)h.nnz, &h.device_bytes), "cudaMalloc(ci)");
@@ -196,10 +203,12 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
     pava_opts o;
     memset(&o, 0, sizeof(o));
     if (opts) o = *opts;
-    if (o.precision != PAVA_PREC_FP64)
-        return fail(PAVA_E_UNSUPPORTED_VALUE_TYPE, "precision not supported by this format");
-    if (o.index_mode != PAVA_INDEX_I32)
-        return fail(PAVA_E_UNSUPPORTED_PARAMS, "index mode not supported by this format");
+    if (o.precision != PAVA_PREC_FP64 && o.precision != PAVA_PREC_FP32C)
+        return fail(PAVA_E_UNSUPPORTED_VALUE_TYPE, "unknown precision");
+    if (o.index_mode != PAVA_INDEX_I32 && o.index_mode != PAVA_INDEX_DELTA16)
+        return fail(PAVA_E_UNSUPPORTED_PARAMS, "unknown index mode");
+    if (format == PAVA_FORMAT_CSR && (o.precision != PAVA_PREC_FP64 || o.index_mode != PAVA_INDEX_I32))
+        return fail(PAVA_E_UNSUPPORTED_VALUE_TYPE, "the plain CSR form is FP64 with 32-bit columns");
 
     pava_handle *H = new (std::nothrow) pava_handle();
     if (!H) return fail(PAVA_E_NOMEM, "host allocation failed");

@@ -15,35 +15,46 @@
 //  * empty rows are given one zero element in column -1 (see k_cvr.cu), so every row of a
 //    tile is consecutive and no descriptor-offset table (format_avx512.h:271-363) is needed.
 //  * a warp walks G consecutive tiles (a chunk) carrying the open row in registers; the
-//    chunk's shared first/last rows go to the carry slots combined by k_fixup.cu, the
+//    chunk's shared first/last rows go to the carry slots combined by k_support.cu, the
 //    deterministic form of the calibrator (csr5_spmv_avx512.h:292-308).  The reference's
 //    serial tail partition (:311-342) does not exist: the last tile is padded.
 //
-// Tile t (32*sigma elements, element (lane l, step i) = original position t*32*sigma +
-// l*sigma + i):
-//   values  at t*32*sigma + (i/VP)*32*VP + VP*l + i%VP
-//   columns at t*32*sigma + (i/CP)*32*CP + CP*l + i%CP
+// Tile t (32*sigma elements; element (lane l, step i) = original position t*32*sigma +
+// l*sigma + i) holds its values and columns in the 4-step block layout of k_stream.cuh, so a
+// chunk of G tiles is one run of G*sigma/4 blocks;
 //   desc[t*32 + l]  bit i: element (l, i) is the first element of a row
 //   tile_ptr[t]     row of element (0, 0)
 
+#include "k_stream.cuh"
 #include "pava_internal.h"
 
 namespace pava {
 
 namespace {
 
-template <int VP, int CP, typename VT>
+template <typename IT> __device__ __forceinline__ IT enc_col(int col, int r_first, int *ovf);
+template <> __device__ __forceinline__ int enc_col<int>(int col, int, int *) { return col; }
+template <> __device__ __forceinline__ short enc_col<short>(int col, int r_first, int *ovf) {
+    if (col < 0) return DELTA_NONE;
+    const int d = col - r_first;
+    if (d < -32767 || d > 32767) { atomicOr(ovf, 1); return DELTA_NONE; }
+    return (short)d;
+}
+
+template <typename VT, typename IT>
 __global__ void __launch_bounds__(256)
 csr5_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                     const double *__restrict__ v, const int *__restrict__ arp, int m,
-                    long long ntiles, int sigma, VT *__restrict__ vals, int *__restrict__ cols,
-                    unsigned *__restrict__ desc, int *__restrict__ tile_ptr) {
+                    long long ntiles, int sigma, int G, VT *__restrict__ vals,
+                    IT *__restrict__ cols, unsigned *__restrict__ desc,
+                    int *__restrict__ tile_ptr, int *ovf) {
     const int lane = threadIdx.x & 31;
     const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (t >= ntiles) return;
-    const long long tbase = t * 32LL * sigma;
-    const long long e0 = tbase + (long long)lane * sigma;
     const int nr = m + 2;
+    const long long tbase = t * 32LL * sigma;
+    const int r_first = upper_bound_m1(arp, nr, (t / G) * 32LL * sigma * G);  // chunk's first row
+    const long long e0 = tbase + (long long)lane * sigma;
     int row = upper_bound_m1(arp, nr, e0);
     if (lane == 0) tile_ptr[t] = row;
     int rbase = 0;
@@ -71,8 +82,8 @@ csr5_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             val = v[e + rbase];
             col = ci[e + rbase];
         }
-        vals[tbase + (i / VP) * 32 * VP + VP * lane + (i % VP)] = (VT)val;
-        cols[tbase + (i / CP) * 32 * CP + CP * lane + (i % CP)] = col;
+        vals[tbase + vals_offset<VT>(i, lane)] = (VT)val;
+        cols[tbase + cols_offset(i, lane)] = enc_col<IT>(col, r_first, ovf);
     }
     desc[t * 32 + lane] = F;
 }
@@ -93,21 +104,25 @@ __global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long n
     hdr[c].aux = 0;
 }
 
+#ifndef PAVA_CSR5_MINB
+#define PAVA_CSR5_MINB 3
+#endif
 constexpr int SPMV_WARPS = 8;
 
-// CSR5 SpMV, FP64: one warp per chunk of G tiles of 32 x SIGMA elements.
-template <int SIGMA>
-__global__ void __launch_bounds__(SPMV_WARPS * 32)
-csr5_spmv_f64_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_ptr,
-                     const unsigned *__restrict__ desc, const double *__restrict__ vals,
-                     const int *__restrict__ cols, const double *__restrict__ x,
-                     double *__restrict__ y, double *__restrict__ carry_head,
-                     double *__restrict__ carry_tail, long long nchunks, int G, int m) {
-    constexpr int TE = 32 * SIGMA;  // elements per tile
-    constexpr int NQ = SIGMA / 4;   // 4-step groups per tile
+// CSR5 SpMV: one warp per chunk of G tiles, walked as one pipelined run of 4-step blocks
+// (values two blocks ahead, columns three, x one); tile descriptors one tile ahead.
+template <int SIGMA, typename VT, typename IT>
+__global__ void __launch_bounds__(SPMV_WARPS * 32, PAVA_CSR5_MINB)
+csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_ptr,
+                 const unsigned *__restrict__ desc, const VT *__restrict__ vals,
+                 const IT *__restrict__ cols, const VT *__restrict__ x,
+                 double *__restrict__ y, double *__restrict__ carry_head,
+                 double *__restrict__ carry_tail, long long nchunks, int G, int m) {
+    constexpr int NBT = SIGMA / 4;  // blocks per tile
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
     const long long nwarps = (long long)gridDim.x * SPMV_WARPS;
+    (void)w;
 
     for (long long c = (long long)blockIdx.x * SPMV_WARPS + w; c < nchunks; c += nwarps) {
         const ChunkHdr H = hdr[c];
@@ -115,63 +130,99 @@ csr5_spmv_f64_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
         const unsigned shared = H.shared;
         int carry_row = (shared & 1u) ? r_first : -1;
         double carry_val = 0.0;
-        for (int tt = 0; tt < G; ++tt) {
-            const long long t = c * G + tt;
-            const int row_start = tile_ptr[t];
-            const unsigned F = ld_stream(desc + t * 32 + lane, pf);
-            const double2 *vb = reinterpret_cast<const double2 *>(vals + t * TE);
-            const int4 *cb = reinterpret_cast<const int4 *>(cols + t * TE);
-            const int b00 = (int)(__shfl_sync(FULL, F, 0) & 1u);
-            const int nst = __popc(F);
-            const int excl = warp_excl_scan(nst, lane);
-            const int total = __shfl_sync(FULL, excl + nst, 31);
-            int rowcur = row_start + excl - b00;  // row open when the lane starts
-            double acc = 0.0, hpiece = 0.0;
-            bool seen = false;
+        const long long t0 = c * G;
+        const VT *vb = vals + t0 * 32 * SIGMA;
+        const IT *cb = cols + t0 * 32 * SIGMA;
+        const int NB = G * NBT;
+
+        CBlk<IT> c1 = CBlk<IT>::load(cb, 1, lane, pf);
+        CBlk<IT> c2 = CBlk<IT>::load(cb, NB > 2 ? 2 : 1, lane, pf);
+        VBlk<VT> v0 = VBlk<VT>::load(vb, 0, lane, pf), v1 = VBlk<VT>::load(vb, 1, lane, pf);
+        VT x0[4];
+        {
+            const CBlk<IT> c0 = CBlk<IT>::load(cb, 0, lane, pf);
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                const int4 cc = ld_stream(cb + q * 32 + lane, pf);
-                const double2 va = ld_stream(vb + (2 * q) * 32 + lane, pf);
-                const double2 vc = ld_stream(vb + (2 * q + 1) * 32 + lane, pf);
-                const double xx[4] = {gather_x(x, cc.x, pl), gather_x(x, cc.y, pl),
-                                      gather_x(x, cc.z, pl), gather_x(x, cc.w, pl)};
-                const double vv[4] = {va.x, va.y, vc.x, vc.y};
+            for (int q = 0; q < 4; ++q) x0[q] = gather_x(x, c0.col(q, r_first), pl);
+        }
+        unsigned Fn = ld_stream(desc + t0 * 32 + lane, pf);
+        int rsn = tile_ptr[t0];
+
+        unsigned F = 0;
+        int rs = 0, b00 = 0, total = 0, rowcur = 0;
+        Acc<VT> acc;
+        double hpiece = 0.0;
+        bool seen = false;
+        int tt = 0;
+#pragma unroll 1
+        for (int blk = 0; blk < NB; ++blk) {
+            CBlk<IT> cn = c2;
+            VBlk<VT> vn = v1;
+            if (blk + 3 < NB) cn = CBlk<IT>::load(cb, blk + 3, lane, pf);
+            if (blk + 2 < NB) vn = VBlk<VT>::load(vb, blk + 2, lane, pf);
+            VT x1[4];
+            if (blk + 1 < NB) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int i = q * 4 + k;
-                    if ((F >> i) & 1u) {
-                        if (seen) {
-                            if (rowcur < m) y[rowcur] = acc;
-                        } else {
-                            hpiece = acc;
-                            seen = true;
-                        }
-                        ++rowcur;
-                        acc = 0.0;
-                    }
-                    acc = fma(vv[k], xx[k], acc);
+                for (int q = 0; q < 4; ++q) x1[q] = gather_x(x, c1.col(q, r_first), pl);
+            }
+            const int qb = blk % NBT;
+            if (qb == 0) {  // tile start
+                F = Fn;
+                rs = rsn;
+                if (tt + 1 < G) {
+                    Fn = ld_stream(desc + (t0 + tt + 1) * 32 + lane, pf);
+                    rsn = tile_ptr[t0 + tt + 1];
                 }
+                b00 = (int)(__shfl_sync(FULL, F, 0) & 1u);
+                const int nst = __popc(F);
+                const int excl = warp_excl_scan(nst, lane);
+                total = __shfl_sync(FULL, excl + nst, 31);
+                rowcur = rs + excl - b00;  // row open when the lane starts
+                acc.reset();
+                hpiece = 0.0;
+                seen = false;
             }
-            if (!seen) hpiece = acc;
-            const double tl = seen ? acc : 0.0;
-            const unsigned sm = __ballot_sync(FULL, seen);
-            const double Hs = seg_suffix(hpiece, !seen, lane);
-            double Hn = __shfl_down_sync(FULL, Hs, 1);
-            if (lane == 31) Hn = 0.0;
-            const double H0 = __shfl_sync(FULL, Hs, 0);
-            if (sm == 0) {
-                carry_val += H0;  // the whole tile continues the open row
-            } else {
-                const int lstar = 31 - __clz(sm);
-                const double own_l = tl + Hn;
-                if (seen && lane != lstar && rowcur < m) y[rowcur] = own_l;
-                const double own = __shfl_sync(FULL, own_l, lstar);
-                if (carry_row >= 0 && lane == 0)
-                    flush_row(carry_row, carry_val + H0, r_first, r_last, shared, c, y,
-                              carry_head, carry_tail, m);
-                carry_row = row_start + total - b00;
-                carry_val = own;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = qb * 4 + q;
+                if ((F >> i) & 1u) {
+                    if (seen) {
+                        if (rowcur < m) y[rowcur] = acc.value();
+                    } else {
+                        hpiece = acc.value();
+                        seen = true;
+                    }
+                    ++rowcur;
+                    acc.reset();
+                }
+                acc.add(v0.get(q), x0[q]);
             }
+            if (qb == NBT - 1) {  // tile end: combine the lanes' open pieces
+                if (!seen) hpiece = acc.value();
+                const double tl = seen ? acc.value() : 0.0;
+                const unsigned sm = __ballot_sync(FULL, seen);
+                const double Hs = seg_suffix(hpiece, !seen, lane);
+                double Hn = __shfl_down_sync(FULL, Hs, 1);
+                if (lane == 31) Hn = 0.0;
+                const double H0 = __shfl_sync(FULL, Hs, 0);
+                if (sm == 0) {
+                    carry_val += H0;  // the whole tile continues the open row
+                } else {
+                    const int lstar = 31 - __clz(sm);
+                    const double own_l = tl + Hn;
+                    if (seen && lane != lstar && rowcur < m) y[rowcur] = own_l;
+                    const double own = __shfl_sync(FULL, own_l, lstar);
+                    if (carry_row >= 0 && lane == 0)
+                        flush_row(carry_row, carry_val + H0, r_first, r_last, shared, c, y,
+                                  carry_head, carry_tail, m);
+                    carry_row = rs + total - b00;
+                    carry_val = own;
+                }
+                ++tt;
+            }
+            c1 = c2; c2 = cn;
+            v0 = v1; v1 = vn;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x0[q] = x1[q];
         }
         if (carry_row >= 0 && lane == 0)
             flush_row(carry_row, carry_val, r_first, r_last, shared, c, y, carry_head,
@@ -179,16 +230,13 @@ csr5_spmv_f64_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
     }
 }
 
-}  // namespace
-
-cudaError_t csr5_convert(Handle &h, const int *rp, const int *ci, const double *v,
-                         cudaStream_t s) {
-    if (h.ntiles <= 0) return cudaSuccess;
+template <typename VT, typename IT>
+cudaError_t convert_t(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,
+                      cudaStream_t s) {
     const long long blocks = (h.ntiles * 32 + 255) / 256;
-    if (h.precision != PAVA_PREC_FP64) return cudaErrorInvalidValue;
-    csr5_convert_kernel<2, 4, double><<<(unsigned)blocks, 256, 0, s>>>(
-        rp, ci, v, h.arp, h.m, h.ntiles, h.sigma, (double *)h.vals, (int *)h.cols, h.flags,
-        h.tile_ptr);
+    csr5_convert_kernel<VT, IT><<<(unsigned)blocks, 256, 0, s>>>(
+        rp, ci, v, h.arp, h.m, h.ntiles, h.sigma, h.G, (VT *)h.vals, (IT *)h.cols, h.flags,
+        h.tile_ptr, ovf);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     chunk_hdr_kernel<<<(unsigned)((h.nchunks + 255) / 256), 256, 0, s>>>(
@@ -196,27 +244,48 @@ cudaError_t csr5_convert(Handle &h, const int *rp, const int *ci, const double *
     return cudaGetLastError();
 }
 
-cudaError_t csr5_spmv(const Handle &h, const void *x, void *y, cudaStream_t s) {
-    if (h.nchunks <= 0) return cudaSuccess;
-    if (h.precision != PAVA_PREC_FP64) return cudaErrorInvalidValue;
+template <int SG, typename VT, typename IT>
+void launch_sg(const Handle &h, unsigned grid, const void *x, void *y, cudaStream_t s) {
+    csr5_spmv_kernel<SG, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
+        (const ChunkHdr *)h.meta, h.tile_ptr, h.flags, (const VT *)h.vals, (const IT *)h.cols,
+        (const VT *)x, (double *)y, h.carry_head, h.carry_tail, h.nchunks, h.G, h.m);
+}
+
+template <typename VT, typename IT>
+cudaError_t spmv_t(const Handle &h, const void *x, void *y, cudaStream_t s) {
     const long long want = (h.nchunks + SPMV_WARPS - 1) / SPMV_WARPS;
-    const long long cap = (long long)h.sm_count * 8;
+    const long long cap = (long long)h.sm_count * PAVA_CSR5_MINB;
     const unsigned grid = (unsigned)(want < cap ? want : cap);
-#define PAVA_CSR5_LAUNCH(SG)                                                                \
-    csr5_spmv_f64_kernel<SG><<<grid, SPMV_WARPS * 32, 0, s>>>(                              \
-        (const ChunkHdr *)h.meta, h.tile_ptr, h.flags, (const double *)h.vals,              \
-        (const int *)h.cols, (const double *)x, (double *)y, h.carry_head, h.carry_tail,    \
-        h.nchunks, h.G, h.m)
     switch (h.sigma) {
-        case 8: PAVA_CSR5_LAUNCH(8); break;
-        case 12: PAVA_CSR5_LAUNCH(12); break;
-        case 16: PAVA_CSR5_LAUNCH(16); break;
-        case 24: PAVA_CSR5_LAUNCH(24); break;
-        case 32: PAVA_CSR5_LAUNCH(32); break;
+        case 8: launch_sg<8, VT, IT>(h, grid, x, y, s); break;
+        case 12: launch_sg<12, VT, IT>(h, grid, x, y, s); break;
+        case 16: launch_sg<16, VT, IT>(h, grid, x, y, s); break;
+        case 24: launch_sg<24, VT, IT>(h, grid, x, y, s); break;
+        case 32: launch_sg<32, VT, IT>(h, grid, x, y, s); break;
         default: return cudaErrorInvalidValue;
     }
-#undef PAVA_CSR5_LAUNCH
     return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t csr5_convert(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,
+                         cudaStream_t s) {
+    if (h.ntiles <= 0) return cudaSuccess;
+    const bool f32 = h.precision == PAVA_PREC_FP32C, d16 = h.index_mode == PAVA_INDEX_DELTA16;
+    if (!f32 && !d16) return convert_t<double, int>(h, rp, ci, v, ovf, s);
+    if (!f32 && d16) return convert_t<double, short>(h, rp, ci, v, ovf, s);
+    if (f32 && !d16) return convert_t<float, int>(h, rp, ci, v, ovf, s);
+    return convert_t<float, short>(h, rp, ci, v, ovf, s);
+}
+
+cudaError_t csr5_spmv(const Handle &h, const void *x, void *y, cudaStream_t s) {
+    if (h.nchunks <= 0) return cudaSuccess;
+    const bool f32 = h.precision == PAVA_PREC_FP32C, d16 = h.index_mode == PAVA_INDEX_DELTA16;
+    if (!f32 && !d16) return spmv_t<double, int>(h, x, y, s);
+    if (!f32 && d16) return spmv_t<double, short>(h, x, y, s);
+    if (f32 && !d16) return spmv_t<float, int>(h, x, y, s);
+    return spmv_t<float, short>(h, x, y, s);
 }
 
 }  // namespace pava

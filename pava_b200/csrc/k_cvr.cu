@@ -9,25 +9,25 @@
 //  * row phase: lane k starts on row r_first + k; whenever lanes finish, they take the next
 //    rows in lane order, so a lane's row is r_first + g with g tracked by ballot/popc.  One bit
 //    per element marks the element that ends the lane's current row (the GPU form of the
-//    reference's (position, row) records): the SpMV stores the lane's FMA accumulator into y
+//    reference's (position, row) records): the SpMV stores the lane's accumulator into y
 //    there.  Rows a lane finishes are summed in CSR order, one FMA per element.
 //  * tail: when a lane finishes and no row is left to take, the rest of the chunk -- the open
 //    rows' remaining elements, in row order -- is spread evenly over the 32 lanes (the GPU
 //    form of the reference's stealing).  Partial sums meet in shared memory through a
 //    fixed-order segmented suffix scan, so the result does not depend on timing.
 //  * a chunk's first / last row may continue in the neighbouring chunk; their partial sums go
-//    to per-chunk carry slots that k_fixup.cu adds in chunk order (the reference adds them
+//    to per-chunk carry slots that k_support.cu adds in chunk order (the reference adds them
 //    with `omp atomic`, cvr/cvr.h:1415,1717,1855).
 //
 // Empty rows are given one element of value 0 in column -1 (which reads no x), so that every
 // row is visited and written: y = A x overwrites all of y on every call.  The last chunk is
 // padded with such elements, which belong to a padding row m whose sum is dropped.
 //
-// Layout of chunk c (L = 32*S elements, element (step i, lane k)):
-//   values  at c*L + (i/VP)*32*VP + VP*k + i%VP   (VP values per 16-byte lane load)
-//   columns at c*L + (i/CP)*32*CP + CP*k + i%CP   (CP columns per 16-byte lane load)
+// Streams of chunk c (L = 32*S elements; the 4-step block layout of k_stream.cuh):
+//   values  at c*L + vals_offset(i, k), columns at c*L + cols_offset(i, k)
 //   flags   word w of lane k at c*S + 32*w + k, bit i%32 of word i/32
 
+#include "k_stream.cuh"
 #include "pava_internal.h"
 
 namespace pava {
@@ -49,27 +49,37 @@ __device__ __forceinline__ RowSrc row_src(const int *rp, const int *arp, int m, 
     return r;
 }
 
-template <int VP, int CP, typename VT>
-__device__ __forceinline__ void put_elem(VT *vals, int *cols, long long cbase, int i, int lane,
-                                         const int *ci, const double *v, int e, RowSrc src) {
+template <typename IT> __device__ __forceinline__ IT encode_col(int col, int r_first, int *ovf);
+template <> __device__ __forceinline__ int encode_col<int>(int col, int, int *) { return col; }
+template <> __device__ __forceinline__ short encode_col<short>(int col, int r_first, int *ovf) {
+    if (col < 0) return DELTA_NONE;
+    const int d = col - r_first;
+    if (d < -32767 || d > 32767) { atomicOr(ovf, 1); return DELTA_NONE; }
+    return (short)d;
+}
+
+template <typename VT, typename IT>
+__device__ __forceinline__ void put_elem(VT *vals, IT *cols, long long cbase, int i, int lane,
+                                         const int *ci, const double *v, int e, RowSrc src,
+                                         int r_first, int *ovf) {
     double val = 0.0;
     int col = -1;
     if (!src.dummy) {
         val = v[e + src.base];
         col = ci[e + src.base];
     }
-    vals[cbase + (i / VP) * 32 * VP + VP * lane + (i % VP)] = (VT)val;
-    cols[cbase + (i / CP) * 32 * CP + CP * lane + (i % CP)] = col;
+    vals[cbase + vals_offset<VT>(i, lane)] = (VT)val;
+    cols[cbase + cols_offset(i, lane)] = encode_col<IT>(col, r_first, ovf);
 }
 
 constexpr int CONV_WARPS = 4;
 
-template <int VP, int CP, typename VT>
+template <typename VT, typename IT>
 __global__ void __launch_bounds__(CONV_WARPS * 32)
 cvr_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                    const double *__restrict__ v, const int *__restrict__ arp, int m,
-                   long long nchunks, int S, VT *__restrict__ vals, int *__restrict__ cols,
-                   unsigned *__restrict__ flags, CvrMeta *__restrict__ meta) {
+                   long long nchunks, int S, VT *__restrict__ vals, IT *__restrict__ cols,
+                   unsigned *__restrict__ flags, CvrMeta *__restrict__ meta, int *ovf) {
     __shared__ int s_len[CONV_WARPS][64];
     __shared__ int s_src[CONV_WARPS][64];
     __shared__ int s_row[CONV_WARPS][64];
@@ -111,7 +121,7 @@ cvr_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             }
             next_g += __popc(b);
         }
-        put_elem<VP, CP>(vals, cols, s, i, lane, ci, v, cur, src);
+        put_elem<VT, IT>(vals, cols, s, i, lane, ci, v, cur, src, r_first, ovf);
         ++cur;
         --rem;
         if (rem == 0) fword |= 1u << (i & 31);
@@ -168,7 +178,7 @@ cvr_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
         int slen = s_len[w][j], sa = s_src[w][j];
         src = row_src(rp, arp, m, s_row[w][j]);
         for (int t = 0; t < T; ++t, ++i) {
-            put_elem<VP, CP>(vals, cols, s, i, lane, ci, v, sa + off, src);
+            put_elem<VT, IT>(vals, cols, s, i, lane, ci, v, sa + off, src, r_first, ovf);
             ++off;
             const bool slot_end = (off == slen);
             if (slot_end || t == T - 1) fword |= 1u << (i & 31);
@@ -202,20 +212,24 @@ cvr_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
 }
 
 // ---------------------------------------------------------------------------------------
-// CVR SpMV, FP64.  One warp per chunk (grid-stride), 8 steps per loop trip: two int4 column
-// loads, four double2 value loads and one flag word per lane, with the next trip's streams
-// requested before this trip's x gathers are consumed.
+// CVR SpMV.  One warp per chunk (grid-stride).  The chunk is walked in 4-step blocks with a
+// software pipeline: value and flag streams are requested two blocks ahead, column streams
+// three blocks ahead, and the x gathers one block ahead of the block being summed, so each
+// lane keeps several 16-byte stream loads and four gathers in flight.
+#ifndef PAVA_CVR_MINB
+#define PAVA_CVR_MINB 2
+#endif
 constexpr int SPMV_WARPS = 8;
 
-template <int S>
-__global__ void __launch_bounds__(SPMV_WARPS * 32)
-cvr_spmv_f64_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ flags,
-                    const double *__restrict__ vals, const int *__restrict__ cols,
-                    const double *__restrict__ x, double *__restrict__ y,
-                    double *__restrict__ carry_head, double *__restrict__ carry_tail,
-                    long long nchunks, int m) {
+template <int S, typename VT, typename IT>
+__global__ void __launch_bounds__(SPMV_WARPS * 32, PAVA_CVR_MINB)
+cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ flags,
+                const VT *__restrict__ vals, const IT *__restrict__ cols,
+                const VT *__restrict__ x, double *__restrict__ y,
+                double *__restrict__ carry_head, double *__restrict__ carry_tail,
+                long long nchunks, int m) {
     constexpr int L = 32 * S;
-    constexpr int NB = S / 8;
+    constexpr int NB = S / 4;
     __shared__ double s_tail[SPMV_WARPS][64];
     __shared__ int s_row[SPMV_WARPS][64];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -229,51 +243,54 @@ cvr_spmv_f64_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict
         const int r_last = r_first + M->h.nrows - 1;
         const unsigned shared = M->h.shared;
         const int i_t = M->i_t;
-        const double2 *vb = reinterpret_cast<const double2 *>(vals + c * L);
-        const int4 *cb = reinterpret_cast<const int4 *>(cols + c * L);
+        const VT *vb = vals + c * L;
+        const IT *cb = cols + c * L;
         const unsigned *fb = flags + c * S;
+        auto LF = [&](int b) { return ld_flag(fb + ((4 * b) >> 5) * 32 + lane); };
 
-        double acc = 0.0;
+        Acc<VT> acc;
         int g = lane, next_g = 32;
         int slot = 0, nfrag = 0, last_nfrag = 0;
         bool cont = false;
         double cin = 0.0, last = 0.0;
 
-        int4 c0 = ld_stream(cb + lane, pf), c1 = ld_stream(cb + 32 + lane, pf);
-        double2 v0 = ld_stream(vb + lane, pf), v1 = ld_stream(vb + 32 + lane, pf);
-        double2 v2 = ld_stream(vb + 64 + lane, pf), v3 = ld_stream(vb + 96 + lane, pf);
-        unsigned fw = ld_stream(fb + lane, pf);
+        // prologue: x of block 0, values/flags of blocks 0-1, columns of blocks 1-2
+        CBlk<IT> c1 = CBlk<IT>::load(cb, 1, lane, pf), c2 = CBlk<IT>::load(cb, 2, lane, pf);
+        VBlk<VT> v0 = VBlk<VT>::load(vb, 0, lane, pf), v1 = VBlk<VT>::load(vb, 1, lane, pf);
+        unsigned f0 = LF(0), f1 = LF(1);
+        VT x0[4];
+        {
+            const CBlk<IT> c0 = CBlk<IT>::load(cb, 0, lane, pf);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x0[q] = gather_x(x, c0.col(q, r_first), pl);
+        }
 #pragma unroll 1
         for (int blk = 0; blk < NB; ++blk) {
-            const int i0 = blk * 8;
-            int4 nc0, nc1;
-            double2 nv0, nv1, nv2, nv3;
-            unsigned nfw = fw;
-            if (blk + 1 < NB) {
-                nc0 = ld_stream(cb + (2 * blk + 2) * 32 + lane, pf);
-                nc1 = ld_stream(cb + (2 * blk + 3) * 32 + lane, pf);
-                nv0 = ld_stream(vb + (4 * blk + 4) * 32 + lane, pf);
-                nv1 = ld_stream(vb + (4 * blk + 5) * 32 + lane, pf);
-                nv2 = ld_stream(vb + (4 * blk + 6) * 32 + lane, pf);
-                nv3 = ld_stream(vb + (4 * blk + 7) * 32 + lane, pf);
-                if (((i0 + 8) & 31) == 0) nfw = ld_stream(fb + ((i0 + 8) >> 5) * 32 + lane, pf);
+            CBlk<IT> cn = c2;
+            VBlk<VT> vn = v1;
+            unsigned fn = f1;
+            if (blk + 3 < NB) cn = CBlk<IT>::load(cb, blk + 3, lane, pf);
+            if (blk + 2 < NB) {
+                vn = VBlk<VT>::load(vb, blk + 2, lane, pf);
+                fn = LF(blk + 2);
             }
-            const int cc[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-            const double vv[8] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y, v3.x, v3.y};
-            double xx[8];
+            VT x1[4];
+            if (blk + 1 < NB) {
 #pragma unroll
-            for (int q = 0; q < 8; ++q) xx[q] = gather_x(x, cc[q], pl);
+                for (int q = 0; q < 4; ++q) x1[q] = gather_x(x, c1.col(q, r_first), pl);
+            }
+            const unsigned fw = f0;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int i = i0 + q;
+            for (int q = 0; q < 4; ++q) {
+                const int i = blk * 4 + q;
                 const bool f = (fw >> (i & 31)) & 1u;
                 if (i < i_t) {
-                    acc = fma(vv[q], xx[q], acc);
+                    acc.add(v0.get(q), x0[q]);
                     const unsigned bal = __ballot_sync(FULL, f);
                     if (f) {
-                        flush_row(r_first + g, acc, r_first, r_last, shared, c, y, carry_head,
-                                  carry_tail, m);
-                        acc = 0.0;
+                        flush_row(r_first + g, acc.value(), r_first, r_last, shared, c, y,
+                                  carry_head, carry_tail, m);
+                        acc.reset();
                         g = next_g + __popc(bal & lt);
                     }
                     next_g += __popc(bal);
@@ -284,29 +301,32 @@ cvr_spmv_f64_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict
                         __syncwarp();
                         const int pk = M->park[lane];
                         if (pk != 0xff) {
-                            s_tail[w][pk] = acc;
+                            s_tail[w][pk] = acc.value();
                             s_row[w][pk] = r_first + g;
                         }
-                        acc = 0.0;
+                        acc.reset();
                         slot = M->first_slot[lane];
                         cont = (M->cont >> lane) & 1u;
                         nfrag = 0;
                         __syncwarp();
                     }
-                    acc = fma(vv[q], xx[q], acc);
+                    acc.add(v0.get(q), x0[q]);
                     if (f) {
-                        if (i == S - 1) { last = acc; last_nfrag = nfrag; }
-                        else if (nfrag == 0 && cont) cin = acc;
-                        else s_tail[w][slot] += acc;  // a fragment that starts in this lane
+                        const double a = acc.value();
+                        if (i == S - 1) { last = a; last_nfrag = nfrag; }
+                        else if (nfrag == 0 && cont) cin = a;
+                        else s_tail[w][slot] += a;  // a fragment that starts in this lane
                         ++slot;
                         ++nfrag;
-                        acc = 0.0;
+                        acc.reset();
                     }
                 }
             }
-            c0 = nc0; c1 = nc1;
-            v0 = nv0; v1 = nv1; v2 = nv2; v3 = nv3;
-            fw = nfw;
+            c1 = c2; c2 = cn;
+            v0 = v1; v1 = vn;
+            f0 = f1; f1 = fn;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x0[q] = x1[q];
         }
         if (i_t < S) {
             // combine fragments that continue across lanes, then store the tail rows
@@ -329,40 +349,65 @@ cvr_spmv_f64_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict
     }
 }
 
-}  // namespace
-
-cudaError_t cvr_convert(Handle &h, const int *rp, const int *ci, const double *v,
-                        cudaStream_t s) {
+template <typename VT, typename IT>
+cudaError_t convert_t(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,
+                      cudaStream_t s) {
     const long long blocks = (h.nchunks + CONV_WARPS - 1) / CONV_WARPS;
-    if (blocks <= 0) return cudaSuccess;
-    if (h.precision == PAVA_PREC_FP64) {
-        cvr_convert_kernel<2, 4, double><<<(unsigned)blocks, CONV_WARPS * 32, 0, s>>>(
-            rp, ci, v, h.arp, h.m, h.nchunks, h.S, (double *)h.vals, (int *)h.cols, h.flags,
-            (CvrMeta *)h.meta);
-    } else {
-        return cudaErrorInvalidValue;
+    cvr_convert_kernel<VT, IT><<<(unsigned)blocks, CONV_WARPS * 32, 0, s>>>(
+        rp, ci, v, h.arp, h.m, h.nchunks, h.S, (VT *)h.vals, (IT *)h.cols, h.flags,
+        (CvrMeta *)h.meta, ovf);
+    return cudaGetLastError();
+}
+
+template <typename VT, typename IT>
+cudaError_t spmv_t(const Handle &h, const void *x, void *y, cudaStream_t s) {
+    const long long want = (h.nchunks + SPMV_WARPS - 1) / SPMV_WARPS;
+    const long long cap = (long long)h.sm_count * PAVA_CVR_MINB;
+    const unsigned grid = (unsigned)(want < cap ? want : cap);
+    const CvrMeta *meta = (const CvrMeta *)h.meta;
+    const VT *xv = (const VT *)x;
+    double *yv = (double *)y;
+    switch (h.S) {
+        case 32:
+            cvr_spmv_kernel<32, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
+                meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, yv, h.carry_head,
+                h.carry_tail, h.nchunks, h.m);
+            break;
+        case 64:
+            cvr_spmv_kernel<64, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
+                meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, yv, h.carry_head,
+                h.carry_tail, h.nchunks, h.m);
+            break;
+        case 128:
+            cvr_spmv_kernel<128, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
+                meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, yv, h.carry_head,
+                h.carry_tail, h.nchunks, h.m);
+            break;
+        default:
+            return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
+}  // namespace
+
+cudaError_t cvr_convert(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,
+                        cudaStream_t s) {
+    if (h.nchunks <= 0) return cudaSuccess;
+    const bool f32 = h.precision == PAVA_PREC_FP32C, d16 = h.index_mode == PAVA_INDEX_DELTA16;
+    if (!f32 && !d16) return convert_t<double, int>(h, rp, ci, v, ovf, s);
+    if (!f32 && d16) return convert_t<double, short>(h, rp, ci, v, ovf, s);
+    if (f32 && !d16) return convert_t<float, int>(h, rp, ci, v, ovf, s);
+    return convert_t<float, short>(h, rp, ci, v, ovf, s);
+}
+
 cudaError_t cvr_spmv(const Handle &h, const void *x, void *y, cudaStream_t s) {
     if (h.nchunks <= 0) return cudaSuccess;
-    const long long want = (h.nchunks + SPMV_WARPS - 1) / SPMV_WARPS;
-    const long long cap = (long long)h.sm_count * 8;
-    const unsigned grid = (unsigned)(want < cap ? want : cap);
-    if (h.precision != PAVA_PREC_FP64) return cudaErrorInvalidValue;
-#define PAVA_CVR_LAUNCH(SV)                                                                 \
-    cvr_spmv_f64_kernel<SV><<<grid, SPMV_WARPS * 32, 0, s>>>(                               \
-        (const CvrMeta *)h.meta, h.flags, (const double *)h.vals, (const int *)h.cols,      \
-        (const double *)x, (double *)y, h.carry_head, h.carry_tail, h.nchunks, h.m)
-    switch (h.S) {
-        case 32: PAVA_CVR_LAUNCH(32); break;
-        case 64: PAVA_CVR_LAUNCH(64); break;
-        case 128: PAVA_CVR_LAUNCH(128); break;
-        default: return cudaErrorInvalidValue;
-    }
-#undef PAVA_CVR_LAUNCH
-    return cudaGetLastError();
+    const bool f32 = h.precision == PAVA_PREC_FP32C, d16 = h.index_mode == PAVA_INDEX_DELTA16;
+    if (!f32 && !d16) return spmv_t<double, int>(h, x, y, s);
+    if (!f32 && d16) return spmv_t<double, short>(h, x, y, s);
+    if (f32 && !d16) return spmv_t<float, int>(h, x, y, s);
+    return spmv_t<float, short>(h, x, y, s);
 }
 
 }  // namespace pava

@@ -1,0 +1,112 @@
+// Stream blocks shared by the CVR and CSR5 SpMV kernels.
+//
+// Both formats store a warp chunk as a sequence of 4-step blocks of 128 elements: element
+// (step i, lane k) of block b sits at chunk_base + b*128 + 4k + (i%4) for values held as FP32
+// or columns of either width, and at chunk_base + b*128 + 64*(i%4 / 2) + 2k + (i%2) for FP64
+// values.  Each lane therefore reads one 16-byte vector per block per stream (8 bytes for the
+// 16-bit columns), and a warp reads whole 128-byte lines.
+//
+// Value forms:  double -- FP64 values and x, FMA accumulation;
+//               float  -- FP32 values and x, compensated accumulation (TwoProduct by FMA,
+//                         TwoSum), the sum and its correction widened to FP64 at the end.
+// Column forms: int    -- 32-bit columns;
+//               short  -- 16-bit offsets from the chunk's first row (col = r_first + d), with
+//                         d = -32768 marking an element that reads no x.
+#pragma once
+#include "pava_common.cuh"
+
+namespace pava {
+
+constexpr short DELTA_NONE = -32768;
+
+template <typename VT> struct VBlk;
+template <> struct VBlk<double> {
+    double2 a, b;
+    __device__ __forceinline__ double get(int q) const {
+        return q == 0 ? a.x : q == 1 ? a.y : q == 2 ? b.x : b.y;
+    }
+    __device__ __forceinline__ static VBlk load(const double *base, int blk, int lane, uint64_t pol) {
+        const double2 *p = reinterpret_cast<const double2 *>(base);
+        VBlk r;
+        r.a = ld_stream(p + (2 * blk) * 32 + lane, pol);
+        r.b = ld_stream(p + (2 * blk + 1) * 32 + lane, pol);
+        return r;
+    }
+};
+template <> struct VBlk<float> {
+    float4 a;
+    __device__ __forceinline__ float get(int q) const {
+        return q == 0 ? a.x : q == 1 ? a.y : q == 2 ? a.z : a.w;
+    }
+    __device__ __forceinline__ static VBlk load(const float *base, int blk, int lane, uint64_t pol) {
+        VBlk r;
+        r.a = ld_stream(reinterpret_cast<const float4 *>(base) + blk * 32 + lane, pol);
+        return r;
+    }
+};
+
+template <typename IT> struct CBlk;
+template <> struct CBlk<int> {
+    int4 a;
+    __device__ __forceinline__ int col(int q, int) const {
+        return q == 0 ? a.x : q == 1 ? a.y : q == 2 ? a.z : a.w;
+    }
+    __device__ __forceinline__ static CBlk load(const int *base, int blk, int lane, uint64_t pol) {
+        CBlk r;
+        r.a = ld_stream(reinterpret_cast<const int4 *>(base) + blk * 32 + lane, pol);
+        return r;
+    }
+};
+template <> struct CBlk<short> {
+    uint2 a;
+    __device__ __forceinline__ int col(int q, int r_first) const {
+        const unsigned w = q < 2 ? a.x : a.y;
+        const int d = (q & 1) ? ((int)w >> 16) : ((int)(w << 16) >> 16);
+        return d == DELTA_NONE ? -1 : r_first + d;
+    }
+    __device__ __forceinline__ static CBlk load(const short *base, int blk, int lane, uint64_t pol) {
+        CBlk r;
+        r.a = ld_stream(reinterpret_cast<const uint2 *>(base) + blk * 32 + lane, pol);
+        return r;
+    }
+};
+
+// Element offset inside a chunk's value / column stream for (step i, lane k).
+template <typename VT>
+__host__ __device__ __forceinline__ long long vals_offset(int i, int k) {
+    if (sizeof(VT) == 8) return (long long)(i >> 1) * 64 + 2 * k + (i & 1);
+    return (long long)(i >> 2) * 128 + 4 * k + (i & 3);
+}
+__host__ __device__ __forceinline__ long long cols_offset(int i, int k) {
+    return (long long)(i >> 2) * 128 + 4 * k + (i & 3);
+}
+
+template <typename VT> struct Acc;
+template <> struct Acc<double> {
+    double s = 0.0;
+    __device__ __forceinline__ void add(double v, double x) { s = fma(v, x, s); }
+    __device__ __forceinline__ double value() const { return s; }
+    __device__ __forceinline__ void reset() { s = 0.0; }
+};
+template <> struct Acc<float> {
+    float s = 0.f, c = 0.f;
+    __device__ __forceinline__ void add(float v, float x) {
+        const float p = v * x;
+        const float e = fmaf(v, x, -p);  // v*x = p + e exactly
+        const float t = s + p;           // TwoSum(s, p) = t + err exactly
+        const float z = t - s;
+        const float err = (s - (t - z)) + (p - z);
+        s = t;
+        c += err + e;
+    }
+    __device__ __forceinline__ double value() const { return (double)s + (double)c; }
+    __device__ __forceinline__ void reset() { s = 0.f; c = 0.f; }
+};
+
+__device__ __forceinline__ unsigned ld_flag(const unsigned *p) {
+    unsigned r;
+    asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(r) : "l"(p));
+    return r;
+}
+
+}  // namespace pava

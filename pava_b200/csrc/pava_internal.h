@@ -61,11 +61,12 @@ cudaError_t launch_validate(const int *rp, const int *ci, int m, int n, int nnz,
 cudaError_t build_augmented_rowptr(const int *rp, int m, long long padded_total, int *arp,
                                    int *d_nempty, cudaStream_t s);
 
-cudaError_t cvr_convert(Handle &h, const int *rp, const int *ci, const double *v,
+// Conversions set *ovf (device) to 1 when a 16-bit column offset does not fit.
+cudaError_t cvr_convert(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,
                         cudaStream_t s);
 cudaError_t cvr_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
 
-cudaError_t csr5_convert(Handle &h, const int *rp, const int *ci, const double *v,
+cudaError_t csr5_convert(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,
                          cudaStream_t s);
 cudaError_t csr5_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
 

@@ -1,0 +1,108 @@
+"""Profiling driver: converts one benchmark matrix into one or more forms and runs a few SpMVs
+of each, for ncu captures and for separating the cost of the x gathers from the streams.
+
+    python -m pava_b200.profile_run --matrix c2 --variants cvr:steps=128 --reps 3
+    python -m pava_b200.profile_run --matrix c3 \\
+        --variants cvr:steps=64,csr5:sigma=16,cvr:steps=64;precision=1;index_mode=1
+
+Matrices: c1 (512^2 Laplacian), c2 (power-law, 4,194,304 rows), c2local (c2's row lengths and
+values with column j of row r replaced by min(r + j, n-1): the same streams, x gathers that hit
+the same sectors), c3 (128^3 27-point stencil), banded (1,048,576 rows, half-bandwidth 64,
+24 per row).  ``--rows`` shrinks c2 / banded for small captures.  A variant is
+``format:key=value;...`` with the pava_opts keys (steps, sigma, tiles_per_chunk, precision
+0=FP64 / 1=FP32C, index_mode 0=I32 / 1=DELTA16, lanes_per_row).  Prints one JSON line per
+variant with the device time of the SpMV kernel (CUDA events) unless --quiet.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+
+def make_matrix(name, rows):
+    from . import matrices as M
+    if name == "c1":
+        return M.laplace2d(512)
+    if name == "c3":
+        return M.stencil27(128)
+    if name == "banded":
+        return M.banded(rows if rows != 4_194_304 else 1_048_576, 64, 24)
+    if name in ("c2", "c2local"):
+        A = M.powerlaw(rows, seed=1)
+        if name == "c2local":
+            r = np.repeat(np.arange(A.m, dtype=np.int64), np.diff(A.rp))
+            j = np.arange(A.nnz, dtype=np.int64) - np.repeat(A.rp[:-1].astype(np.int64), np.diff(A.rp))
+            A.ci = np.minimum(r + j, A.n - 1).astype(np.int32)
+        return A
+    raise SystemExit(f"unknown matrix {name}")
+
+
+def parse_variants(spec):
+    out = []
+    for item in spec.split(","):
+        fmt, _, rest = item.partition(":")
+        kw = {}
+        for kv in filter(None, rest.split(";")):
+            k, v = kv.split("=")
+            kw[k] = int(v)
+        out.append((fmt, kw))
+    return out
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--matrix", default="c2")
+    p.add_argument("--rows", type=int, default=4_194_304)
+    p.add_argument("--variants", default="cvr:steps=128")
+    p.add_argument("--reps", type=int, default=3)
+    p.add_argument("--quiet", action="store_true")
+    a = p.parse_args()
+
+    import torch
+    from . import _abi
+    from .api import SpMatrix
+    from . import matrices as M
+
+    torch.cuda.set_device(0)
+    _abi.check(_abi.gpu().pava_init(0))
+    A = make_matrix(a.matrix, a.rows)
+    x64 = M.uniform(A.n, seed=1, fp32=True)
+    for fmt, kw in parse_variants(a.variants):
+        prec = kw.get("precision", _abi.PREC_FP64)
+        x = torch.from_numpy(x64).cuda()
+        if prec == _abi.PREC_FP32C:
+            x = x.float()
+        try:
+            mat = SpMatrix(A, fmt, **kw)
+        except _abi.PavaError as e:
+            print(json.dumps({"matrix": a.matrix, "format": fmt, "opts": kw, "error": str(e)}))
+            continue
+        y = torch.empty(A.m, dtype=torch.float64, device="cuda")
+        s = torch.cuda.current_stream().cuda_stream
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(a.reps)]
+        for k in range(a.reps):
+            ev[k][0].record()
+            mat.spmv_raw(x.data_ptr(), y.data_ptr(), s, 1)
+            ev[k][1].record()
+            mat.spmv_raw(x.data_ptr(), y.data_ptr(), s, 2)
+        torch.cuda.synchronize()
+        if not a.quiet:
+            info = mat.info()
+            t = [e0.elapsed_time(e1) for e0, e1 in ev]
+            best = min(t[1:]) if len(t) > 1 else t[0]
+            print(json.dumps({"matrix": a.matrix, "format": fmt, "opts": kw, "m": A.m,
+                              "nnz": A.nnz, "main_ms": t, "best_ms": best,
+                              "alg_GBps": info["alg_bytes"] / (best * 1e-3) / 1e9,
+                              "format_GBps": info["format_bytes"] / (best * 1e-3) / 1e9,
+                              "alg_bytes": info["alg_bytes"],
+                              "format_bytes": info["format_bytes"],
+                              "convert_ms": info["convert_ms"]}), flush=True)
+        mat.close()
+        del mat
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,94 @@
+"""The precision and index-compression forms against the FP64 oracle.
+
+FP32C: values and x stored in FP32 (the matrices and x are drawn FP32-representable, so the
+oracle's FP64 inputs are the exact widenings), FP32 compensated accumulation, FP64 carries.
+Stated bound: relative error <= 1e-9 per row (cancellation-aware denominator).
+DELTA16: 16-bit column offsets from the chunk's first row; the arithmetic is unchanged, so
+FP64 + DELTA16 must equal FP64 + I32 bit for bit."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pava_b200 import _abi
+from pava_b200 import matrices as M
+from pava_b200.api import SpMatrix
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 1e-9
+FORMS = [("cvr", dict(steps=64)), ("cvr", dict(steps=128)), ("csr5", dict(sigma=16)),
+         ("csr5", dict(sigma=32, tiles_per_chunk=2))]
+FID = ["cvr64", "cvr128", "csr5s16", "csr5s32"]
+
+
+def _run(torch, A, x, fmt, precision, index_mode, **kw):
+    mat = SpMatrix(A, fmt, precision=precision, index_mode=index_mode, **kw)
+    dt = torch.float32 if precision == _abi.PREC_FP32C else torch.float64
+    xd = torch.from_numpy(x).to("cuda", dt)
+    y = torch.full((A.m,), float("nan"), dtype=torch.float64, device="cuda")
+    mat.spmv(xd, y)
+    return y.cpu().numpy(), mat
+
+
+@pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
+@pytest.mark.parametrize("index_mode", [_abi.INDEX_I32, _abi.INDEX_DELTA16], ids=["i32", "d16"])
+def test_fp32c_stencil(cuda, fmt, kw, index_mode):
+    A = M.stencil27(40, seed=2)
+    x = M.uniform(A.n, seed=3, fp32=True)
+    y, _ = _run(cuda, A, x, fmt, _abi.PREC_FP32C, index_mode, **kw)
+    yr, ab = O.csr_ref(A.rp, A.ci, A.v, x)
+    bad, mx, mean = O.rel_error(y, yr, ab, TOL32)
+    assert bad == 0, (mx, mean)
+    # compensated accumulation is far better than the bound
+    assert mx < 1e-12
+
+
+@pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
+def test_fp32c_irregular(cuda, fmt, kw):
+    A = M.powerlaw(200_000, mean=16.0, cap=50_000, seed=5)
+    A.v = A.v.astype(np.float32).astype(np.float64)
+    x = M.uniform(A.n, seed=6, fp32=True)
+    y, _ = _run(cuda, A, x, fmt, _abi.PREC_FP32C, _abi.INDEX_I32, **kw)
+    yr, ab = O.csr_ref(A.rp, A.ci, A.v, x)
+    bad, mx, _ = O.rel_error(y, yr, ab, TOL32)
+    assert bad == 0, mx
+
+
+@pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
+def test_fp64_delta16_equals_i32(cuda, fmt, kw):
+    A = M.banded(300_000, 64, 24, seed=7)
+    x = M.uniform(A.n, seed=8)
+    y32, _ = _run(cuda, A, x, fmt, _abi.PREC_FP64, _abi.INDEX_I32, **kw)
+    y16, _ = _run(cuda, A, x, fmt, _abi.PREC_FP64, _abi.INDEX_DELTA16, **kw)
+    assert np.array_equal(y32, y16)
+    yr, ab = O.csr_ref(A.rp, A.ci, A.v, x)
+    assert O.rel_error(y16, yr, ab, 1e-12)[0] == 0
+
+
+def test_delta16_out_of_range_rejected(cuda):
+    A = M.random_csr(50_000, 50_000, 8.0, seed=9)
+    with pytest.raises(_abi.PavaError) as e:
+        SpMatrix(A, "cvr", index_mode=_abi.INDEX_DELTA16)
+    assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
+
+
+def test_fp32c_wrong_x_dtype_rejected(cuda):
+    A = M.laplace2d(32)
+    mat = SpMatrix(A, "cvr", precision=_abi.PREC_FP32C)
+    with pytest.raises(TypeError):
+        mat.spmv(cuda.zeros(A.n, dtype=cuda.float64, device="cuda"))
+
+
+def test_config3_full_size_fp32c_vs_fp64(cuda):
+    """128^3 27-point stencil: FP64 drop-in within 1e-12, FP32C within 1e-9 of the oracle."""
+    A = M.stencil27(128, seed=2)
+    x = M.uniform(A.n, seed=3, fp32=True)
+    yr, ab = O.csr_ref(A.rp, A.ci, A.v, x)
+    y64, m64 = _run(cuda, A, x, "csr5", _abi.PREC_FP64, _abi.INDEX_I32)
+    assert O.rel_error(y64, yr, ab, 1e-12)[0] == 0
+    del m64
+    for fmt in ("cvr", "csr5"):
+        y32, m32 = _run(cuda, A, x, fmt, _abi.PREC_FP32C, _abi.INDEX_DELTA16)
+        bad, mx, mean = O.rel_error(y32, yr, ab, TOL32)
+        assert bad == 0, (fmt, mx, mean)
+        del m32
