@@ -104,6 +104,9 @@ __global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long n
     hdr[c].aux = 0;
 }
 
+#ifndef PAVA_CSR5_MINB32
+#define PAVA_CSR5_MINB32 3
+#endif
 #ifndef PAVA_CSR5_MINB
 #define PAVA_CSR5_MINB 3
 #endif
@@ -112,7 +115,7 @@ constexpr int SPMV_WARPS = 8;
 // CSR5 SpMV: one warp per chunk of G tiles, walked as one pipelined run of 4-step blocks
 // (values two blocks ahead, columns three, x one); tile descriptors one tile ahead.
 template <int SIGMA, typename VT, typename IT>
-__global__ void __launch_bounds__(SPMV_WARPS * 32, PAVA_CSR5_MINB)
+__global__ void __launch_bounds__(SPMV_WARPS * 32, sizeof(VT) == 8 ? PAVA_CSR5_MINB : PAVA_CSR5_MINB32)
 csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_ptr,
                  const unsigned *__restrict__ desc, const VT *__restrict__ vals,
                  const IT *__restrict__ cols, const VT *__restrict__ x,
@@ -254,7 +257,7 @@ void launch_sg(const Handle &h, unsigned grid, const void *x, void *y, cudaStrea
 template <typename VT, typename IT>
 cudaError_t spmv_t(const Handle &h, const void *x, void *y, cudaStream_t s) {
     const long long want = (h.nchunks + SPMV_WARPS - 1) / SPMV_WARPS;
-    const long long cap = (long long)h.sm_count * PAVA_CSR5_MINB;
+    const long long cap = (long long)h.sm_count * (sizeof(VT) == 8 ? PAVA_CSR5_MINB : PAVA_CSR5_MINB32);
     const unsigned grid = (unsigned)(want < cap ? want : cap);
     switch (h.sigma) {
         case 8: launch_sg<8, VT, IT>(h, grid, x, y, s); break;

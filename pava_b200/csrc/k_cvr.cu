@@ -216,13 +216,16 @@ cvr_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
 // software pipeline: value and flag streams are requested two blocks ahead, column streams
 // three blocks ahead, and the x gathers one block ahead of the block being summed, so each
 // lane keeps several 16-byte stream loads and four gathers in flight.
+#ifndef PAVA_CVR_MINB32
+#define PAVA_CVR_MINB32 3
+#endif
 #ifndef PAVA_CVR_MINB
 #define PAVA_CVR_MINB 2
 #endif
 constexpr int SPMV_WARPS = 8;
 
 template <int S, typename VT, typename IT>
-__global__ void __launch_bounds__(SPMV_WARPS * 32, PAVA_CVR_MINB)
+__global__ void __launch_bounds__(SPMV_WARPS * 32, sizeof(VT) == 8 ? PAVA_CVR_MINB : PAVA_CVR_MINB32)
 cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ flags,
                 const VT *__restrict__ vals, const IT *__restrict__ cols,
                 const VT *__restrict__ x, double *__restrict__ y,
@@ -362,7 +365,7 @@ cudaError_t convert_t(Handle &h, const int *rp, const int *ci, const double *v, 
 template <typename VT, typename IT>
 cudaError_t spmv_t(const Handle &h, const void *x, void *y, cudaStream_t s) {
     const long long want = (h.nchunks + SPMV_WARPS - 1) / SPMV_WARPS;
-    const long long cap = (long long)h.sm_count * PAVA_CVR_MINB;
+    const long long cap = (long long)h.sm_count * (sizeof(VT) == 8 ? PAVA_CVR_MINB : PAVA_CVR_MINB32);
     const unsigned grid = (unsigned)(want < cap ? want : cap);
     const CvrMeta *meta = (const CvrMeta *)h.meta;
     const VT *xv = (const VT *)x;
