@@ -129,6 +129,22 @@ pava_status pava_destroy(pava_handle *h);
 const char *pava_last_error(void);
 const char *pava_status_string(int status);
 
+/* y = A x straight from a CSR already in device memory, allocating nothing: for callers that
+ * may not call the CUDA allocator because a host framework owns the device memory and hands
+ * them only pre-allocated buffers (or because their memory budget is already committed), and
+ * so cannot create a handle.  No counterpart in the reference.
+ *   - Scratch: a 1 MiB array compiled into this library (held on every GPU that loads it until
+ *     the process exits), enough for 32,768 chunks of 4,096 nonzeros: nnz above 134,217,728
+ *     returns PAVA_E_TOO_LARGE and launches nothing.
+ *   - The first call on a device looks up the array's device address on the current device
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the array: calls that overlap on the GPU (other streams, other threads)
+ *     race and must be serialised by the caller.  Each call rewrites every slot it reads.
+ *   - The CSR must be valid (non-decreasing row_ptr, row_ptr[m] == nnz, columns in [0, n)); it
+ *     is not checked.  Empty rows get y = 0; results agree with pava_spmv within rounding. */
+pava_status pava_spmv_csr_noalloc(int m, int n, int nnz, const int *row_ptr, const int *col_idx,
+                                  const double *vals, const double *x, double *y, void *stream);
+
 /* Drop-ins for the reference's engine entry points, same signatures and meaning:
  * conduct_cvr (cvr/cvr.h:1953) and conduct_csr5 (csr5/csr5.h:72-74).  Each copies the CSR to
  * the device, converts (timed as the convert column), runs one SpMV into refOut / y (the

@@ -73,6 +73,8 @@ GPU_SYMBOLS = [
     ("pava_destroy", c_int, [c_void_p]),
     ("pava_last_error", c_char_p, []),
     ("pava_status_string", c_char_p, [c_int]),
+    ("pava_spmv_csr_noalloc", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
+                                      c_void_p, c_void_p, c_void_p]),
     ("conduct_cvr_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_int, c_char_p, c_int]),
     ("conduct_csr5_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,

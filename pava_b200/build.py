@@ -23,7 +23,7 @@ LIBDIR = os.path.join(HERE, "lib")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-GPU_SOURCES = ["api.cu", "k_support.cu", "k_cvr.cu", "k_csr5.cu"]
+GPU_SOURCES = ["api.cu", "k_support.cu", "k_cvr.cu", "k_csr5.cu", "noalloc.cu"]
 HOST_SOURCES = ["host/gen.cpp", "host/mtx.cpp"]
 
 
