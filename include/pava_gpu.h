@@ -40,7 +40,7 @@ typedef enum pava_status {
 /* Storage formats.  CSR and CSR5 keep the reference's ANONYMOUSLIB_FORMAT_* values
  * (csr5/detail/common.h:20-22); CVR is cvr/cvr.h's format. */
 typedef enum pava_format {
-    PAVA_FORMAT_CSR = 0,   /* plain CSR, lanes-per-row vector kernel (baseline and checker) */
+    PAVA_FORMAT_CSR = 0,   /* plain CSR, row-group kernel (lanes per row, SpMM, batches) */
     PAVA_FORMAT_CSR5 = 1,  /* CSR5 tiles: 32 lanes x sigma, bit-flag descriptors */
     PAVA_FORMAT_CVR = 3    /* CVR chunks: 32 lanes x S steps, row-completion bits */
 } pava_format;
@@ -73,7 +73,14 @@ typedef struct pava_opts {
     int tiles_per_chunk;  /* CSR5: tiles per warp chunk (default 4) */
     int precision;        /* pava_precision */
     int index_mode;       /* pava_index_mode */
-    int lanes_per_row;    /* CSR: 1, 2, 4, 8, 16 or 32 (default: from the mean row length) */
+    int lanes_per_row;    /* CSR: lanes per row group, 1, 2, 4, 8, 16 or 32 (default: from
+                             the mean row length, or from k for pava_spmm) */
+    int col_lanes;        /* CSR, pava_spmm: lanes of a group across the k right-hand sides,
+                             a power of two <= lanes_per_row (default: from k) */
+    int cols_per_lane;    /* CSR, pava_spmm: right-hand sides per lane, 1, 2 or 4; needs
+                             col_lanes * cols_per_lane >= k (default: from k) */
+    int rows_per_tile;    /* CSR: rows per warp tile of the persistent launch, a multiple of
+                             32 / lanes_per_row (default: 4 row groups) */
 } pava_opts;
 
 typedef struct pava_info {
@@ -109,6 +116,12 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
  * whose repeated calls accumulate into shared rows (cvr/cvr.h:1415; csr5_spmv_avx512.h:277). */
 pava_status pava_spmv(pava_handle *h, const void *x, void *y, void *stream);
 
+/* Y = A X for k right-hand sides: X is n x k and Y is m x k, both row-major with leading
+ * dimensions ldx >= k and ldy >= k (elements), device memory.  CSR handles only (the
+ * row-group kernel; FP64, or FP32C with float X and double Y), 1 <= k <= 128.  The reference
+ * has no multi-vector product; k = 1 equals pava_spmv. */
+pava_status pava_spmm(pava_handle *h, int k, const void *X, long long ldx, void *Y,
+                      long long ldy, void *stream);
 /* pava_spmv split into its launches, for timing one kernel: stage 1 runs the format's SpMV
  * kernel, stage 2 the carry fixup that finishes rows shared between warp chunks (CVR and
  * CSR5; a no-op for CSR), stage 0 both (= pava_spmv).  y is complete only after stage 2.
@@ -144,6 +157,47 @@ const char *pava_status_string(int status);
  *     is not checked.  Empty rows get y = 0; results agree with pava_spmv within rounding. */
 pava_status pava_spmv_csr_noalloc(int m, int n, int nnz, const int *row_ptr, const int *col_idx,
                                   const double *vals, const double *x, double *y, void *stream);
+
+/* ---- Batches of independent matrices ------------------------------------------------
+ * No counterpart in the reference (its benchmark loop runs one matrix at a time,
+ * main.cpp:554-587).  A batch holds the block-diagonal union of `count` matrices: x and y
+ * of the batch are the matrices' x and y concatenated (offsets from pava_batch_layout), so
+ * one SpMV over the union -- one launch, persistent for the CSR form -- serves all of them. */
+typedef struct pava_batch pava_batch;
+/* mats[i] is a CSR (host or device arrays per its on_device flag), validated per matrix.
+ * format < 0 autotunes the union over the built-in candidates (pava_autotune, k = 1) and
+ * keeps the fastest; otherwise format/opts are used as in pava_create.  Sums of rows,
+ * columns and nonzeros must stay below 2^31 (PAVA_E_TOO_LARGE). */
+pava_status pava_batch_create(int count, const pava_csr *mats, int format,
+                              const pava_opts *opts, void *stream, pava_batch **out);
+/* count + 1 prefix offsets of each matrix's x, y and nonzeros in the union (any may be NULL). */
+pava_status pava_batch_layout(const pava_batch *b, long long *x_offsets, long long *y_offsets,
+                              long long *nnz_offsets);
+/* The chosen form and the union's pava_info (any may be NULL). */
+pava_status pava_batch_get(const pava_batch *b, int *format, pava_opts *opts, pava_info *info);
+/* y = U x for the whole batch (x, y device buffers of the union's n and m). */
+pava_status pava_batch_spmv(pava_batch *b, const void *x, void *y, void *stream);
+/* Records the batch SpMV on (x, y) into a CUDA graph owned by the batch (replacing any
+ * earlier one); pava_batch_replay launches it on `stream`. */
+pava_status pava_batch_capture(pava_batch *b, const void *x, void *y);
+pava_status pava_batch_replay(pava_batch *b, void *stream);
+pava_status pava_batch_destroy(pava_batch *b);
+
+/* ---- Exhaustive autotuner ------------------------------------------------------------
+ * Converts A into every built-in candidate form for k right-hand sides and times each (two
+ * warm-up calls, then the median of `reps` CUDA-event timings of the SpMV/SpMM with x and y
+ * already on the device).  Candidates: for k = 1, CVR steps 64/128 and CSR5 sigma 16/32; for
+ * every k, the CSR row-group form over lanes_per_row x col_lanes x cols_per_lane x
+ * rows_per_tile.  entries[0 .. *n_entries) receive every candidate (ms < 0 when it failed,
+ * with its status), *best the index of the fastest.  No counterpart in the reference. */
+typedef struct pava_tune_entry {
+    int format;
+    pava_opts opts;
+    double ms;
+    int status;
+} pava_tune_entry;
+pava_status pava_autotune(const pava_csr *A, int k, int precision, int reps,
+                          pava_tune_entry *entries, int max_entries, int *n_entries, int *best);
 
 /* Drop-ins for the reference's engine entry points, same signatures and meaning:
  * conduct_cvr (cvr/cvr.h:1953) and conduct_csr5 (csr5/csr5.h:72-74).  Each copies the CSR to

@@ -45,7 +45,8 @@ class PavaCsr(ctypes.Structure):
 
 class PavaOpts(ctypes.Structure):
     _fields_ = [("steps", c_int), ("sigma", c_int), ("tiles_per_chunk", c_int),
-                ("precision", c_int), ("index_mode", c_int), ("lanes_per_row", c_int)]
+                ("precision", c_int), ("index_mode", c_int), ("lanes_per_row", c_int),
+                ("col_lanes", c_int), ("cols_per_lane", c_int), ("rows_per_tile", c_int)]
 
 
 class PavaInfo(ctypes.Structure):
@@ -53,6 +54,10 @@ class PavaInfo(ctypes.Structure):
                 ("n", c_int), ("nnz", c_int), ("n_empty", c_int), ("chunks", c_ll),
                 ("elems_per_chunk", c_ll), ("convert_ms", c_dbl), ("device_bytes", c_size_t),
                 ("alg_bytes", c_dbl), ("format_bytes", c_dbl)]
+
+
+class PavaTuneEntry(ctypes.Structure):
+    _fields_ = [("format", c_int), ("opts", PavaOpts), ("ms", c_dbl), ("status", c_int)]
 
 
 class PavaError(RuntimeError):
@@ -68,6 +73,7 @@ GPU_SYMBOLS = [
                             ctypes.POINTER(c_void_p)]),
     ("pava_spmv", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("pava_spmv_stage", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
+    ("pava_spmm", c_int, [c_void_p, c_int, c_void_p, c_ll, c_void_p, c_ll, c_void_p]),
     ("pava_spmv_host", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("pava_get_info", c_int, [c_void_p, ctypes.POINTER(PavaInfo)]),
     ("pava_destroy", c_int, [c_void_p]),
@@ -75,6 +81,18 @@ GPU_SYMBOLS = [
     ("pava_status_string", c_char_p, [c_int]),
     ("pava_spmv_csr_noalloc", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
                                       c_void_p, c_void_p, c_void_p]),
+    ("pava_batch_create", c_int, [c_int, ctypes.POINTER(PavaCsr), c_int,
+                                  ctypes.POINTER(PavaOpts), c_void_p, ctypes.POINTER(c_void_p)]),
+    ("pava_batch_layout", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("pava_batch_get", c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(PavaOpts),
+                               ctypes.POINTER(PavaInfo)]),
+    ("pava_batch_spmv", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("pava_batch_capture", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("pava_batch_replay", c_int, [c_void_p, c_void_p]),
+    ("pava_batch_destroy", c_int, [c_void_p]),
+    ("pava_autotune", c_int, [ctypes.POINTER(PavaCsr), c_int, c_int, c_int,
+                              ctypes.POINTER(PavaTuneEntry), c_int, ctypes.POINTER(c_int),
+                              ctypes.POINTER(c_int)]),
     ("conduct_cvr_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_int, c_char_p, c_int]),
     ("conduct_csr5_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -1,6 +1,10 @@
 """Python mirror of the reference's engine interface, backed by the CUDA engine.
 
-* ``SpMatrix``             -- a converted matrix on the GPU (pava_create / pava_spmv)
+* ``SpMatrix``             -- a converted matrix on the GPU (pava_create / pava_spmv, and
+  pava_spmm for k right-hand sides on the CSR row-group form)
+* ``Batch``                -- many independent matrices as one block-diagonal union, one
+  launch per SpMV, replayable from a CUDA graph (pava_batch_*)
+* ``autotune``             -- exhaustive search over the candidate forms (pava_autotune)
 * ``AnonymousLibHandle``   -- the CSR5 handle of csr5/anonymouslib_avx512.h:14-276 (inputCSR,
   setX, setSigma, asCSR5, spmv, asCSR, destroy), same names, argument meaning and status codes
 * ``conduct_cvr`` / ``conduct_csr5`` -- the engine entry points of cvr/cvr.h:1953 and
@@ -39,8 +43,9 @@ class SpMatrix:
 
     def __init__(self, A: CSR, format: str = "cvr", steps: int = 0, sigma: int = 0,
                  tiles_per_chunk: int = 0, precision: int = _abi.PREC_FP64,
-                 index_mode: int = _abi.INDEX_I32, lanes_per_row: int = 0, stream=None,
-                 device_arrays=None):
+                 index_mode: int = _abi.INDEX_I32, lanes_per_row: int = 0,
+                 col_lanes: int = 0, cols_per_lane: int = 0, rows_per_tile: int = 0,
+                 stream=None, device_arrays=None):
         L = _abi.gpu()
         self.m, self.n, self.nnz = A.m, A.n, A.nnz
         self.format = format
@@ -58,7 +63,8 @@ class SpMatrix:
             csr.col_idx = self._keep[1].ctypes.data
             csr.vals = self._keep[2].ctypes.data
             csr.on_device = 0
-        opts = _abi.PavaOpts(steps, sigma, tiles_per_chunk, precision, index_mode, lanes_per_row)
+        opts = _abi.PavaOpts(steps, sigma, tiles_per_chunk, precision, index_mode, lanes_per_row,
+                             col_lanes, cols_per_lane, rows_per_tile)
         h = _abi.c_void_p()
         _abi.check(L.pava_create(ctypes.byref(csr), FORMATS[format], ctypes.byref(opts),
                                  _abi.c_void_p(_stream_ptr(stream) if stream is not None else None),
@@ -86,6 +92,21 @@ class SpMatrix:
                                         _abi.c_void_p(_stream_ptr(stream))))
         return y
 
+    def spmm(self, X, Y=None, stream=None):
+        """Y = A X for a row-major (n, k) CUDA tensor X (CSR handles); Y is (m, k) float64."""
+        torch = _torch()
+        want = torch.float32 if self.precision == _abi.PREC_FP32C else torch.float64
+        if X.dim() != 2 or X.dtype != want or not X.is_cuda or X.stride(1) != 1:
+            raise TypeError(f"X must be a row-major 2-D CUDA {want} tensor")
+        k = X.shape[1]
+        if Y is None:
+            Y = torch.empty((self.m, k), dtype=torch.float64, device=X.device)
+        if Y.dtype != torch.float64 or Y.dim() != 2 or Y.stride(1) != 1:
+            raise TypeError("Y must be a row-major 2-D CUDA float64 tensor")
+        _abi.check(_abi.gpu().pava_spmm(self._h, k, X.data_ptr(), X.stride(0), Y.data_ptr(),
+                                        Y.stride(0), _abi.c_void_p(_stream_ptr(stream))))
+        return Y
+
     def spmv_raw(self, x_ptr: int, y_ptr: int, stream_ptr: int | None, stage: int = 0) -> None:
         """pava_spmv_stage on raw device pointers: stage 1 = SpMV kernel, 2 = carry fixup,
         0 = both."""
@@ -111,6 +132,125 @@ class SpMatrix:
     def close(self):
         if getattr(self, "_h", None):
             _abi.gpu().pava_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- autotuner and batches ------------------------------------------------------------------
+
+FORMAT_NAMES = {v: k for k, v in FORMATS.items()}
+OPT_KEYS = [f for f, _ in _abi.PavaOpts._fields_]
+
+
+def _csr_struct(A: CSR, keep: list):
+    csr = _abi.PavaCsr()
+    csr.m, csr.n, csr.nnz = A.m, A.n, A.nnz
+    arrs = (np.ascontiguousarray(A.rp, np.int32), np.ascontiguousarray(A.ci, np.int32),
+            np.ascontiguousarray(A.v, np.float64))
+    keep.append(arrs)
+    csr.row_ptr, csr.col_idx, csr.vals = (a.ctypes.data for a in arrs)
+    csr.on_device = 0
+    return csr
+
+
+def _opts_dict(o) -> dict:
+    return {k: getattr(o, k) for k in OPT_KEYS}
+
+
+def autotune(A: CSR, k: int = 1, precision: int = _abi.PREC_FP64, reps: int = 5):
+    """Exhaustive search (pava_autotune): returns (entries, best_index); each entry is a dict
+    with the form's name, its options, the median ms (< 0 if it failed) and the status."""
+    keep = []
+    csr = _csr_struct(A, keep)
+    cap = 128
+    ents = (_abi.PavaTuneEntry * cap)()
+    n, best = _abi.c_int(), _abi.c_int()
+    _abi.check(_abi.gpu().pava_autotune(ctypes.byref(csr), k, precision, reps, ents, cap,
+                                        ctypes.byref(n), ctypes.byref(best)))
+    out = [{"format": FORMAT_NAMES[e.format], "opts": _opts_dict(e.opts), "ms": e.ms,
+            "status": e.status} for e in ents[: n.value]]
+    return out, best.value
+
+
+class Batch:
+    """Many independent CSR matrices as one block-diagonal union on the GPU.
+
+    ``format`` is 'cvr', 'csr5', 'csr' or 'auto' (autotuned over the candidate forms).  x and
+    y of the batch are the matrices' vectors concatenated; ``layout()`` gives the offsets.
+    """
+
+    def __init__(self, mats, format: str = "auto", precision: int = _abi.PREC_FP64, **opts):
+        keep = []
+        arr = (_abi.PavaCsr * len(mats))()
+        for i, A in enumerate(mats):
+            arr[i] = _csr_struct(A, keep)
+        o = _abi.PavaOpts()
+        o.precision = precision
+        for key, val in opts.items():
+            setattr(o, key, val)
+        fmt = -1 if format == "auto" else FORMATS[format]
+        h = _abi.c_void_p()
+        _abi.check(_abi.gpu().pava_batch_create(len(mats), arr, fmt, ctypes.byref(o), None,
+                                                ctypes.byref(h)))
+        self._h = h
+        self.count = len(mats)
+        self.precision = precision
+        xo = np.zeros(self.count + 1, np.int64)
+        yo = np.zeros(self.count + 1, np.int64)
+        zo = np.zeros(self.count + 1, np.int64)
+        _abi.check(_abi.gpu().pava_batch_layout(h, xo.ctypes.data, yo.ctypes.data, zo.ctypes.data))
+        self.x_offsets, self.y_offsets, self.nnz_offsets = xo, yo, zo
+        self.n, self.m, self.nnz = int(xo[-1]), int(yo[-1]), int(zo[-1])
+
+    def chosen(self):
+        f = _abi.c_int()
+        o = _abi.PavaOpts()
+        _abi.check(_abi.gpu().pava_batch_get(self._h, ctypes.byref(f), ctypes.byref(o), None))
+        return FORMAT_NAMES[f.value], _opts_dict(o)
+
+    def info(self) -> dict:
+        inf = _abi.PavaInfo()
+        _abi.check(_abi.gpu().pava_batch_get(self._h, None, None, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in _abi.PavaInfo._fields_}
+
+    def _check_xy(self, x, y):
+        torch = _torch()
+        want = torch.float32 if self.precision == _abi.PREC_FP32C else torch.float64
+        if x.dtype != want or not x.is_cuda or x.numel() < self.n:
+            raise TypeError(f"x must be a CUDA {want} tensor of {self.n} entries")
+        if y.dtype != torch.float64 or not y.is_cuda or y.numel() < self.m:
+            raise TypeError(f"y must be a CUDA float64 tensor of {self.m} entries")
+
+    def spmv(self, x, y=None, stream=None):
+        torch = _torch()
+        if y is None:
+            y = torch.empty(self.m, dtype=torch.float64, device=x.device)
+        self._check_xy(x, y)
+        _abi.check(_abi.gpu().pava_batch_spmv(self._h, x.data_ptr(), y.data_ptr(),
+                                              _abi.c_void_p(_stream_ptr(stream))))
+        return y
+
+    def capture(self, x, y):
+        """Records the SpMV on (x, y) into the batch's CUDA graph."""
+        self._check_xy(x, y)
+        self._graph_xy = (x, y)
+        _abi.check(_abi.gpu().pava_batch_capture(self._h, x.data_ptr(), y.data_ptr()))
+
+    def replay(self, stream=None):
+        _abi.check(_abi.gpu().pava_batch_replay(self._h, _abi.c_void_p(_stream_ptr(stream))))
+
+    def split(self, y):
+        """The per-matrix slices of a batch vector y."""
+        return [y[self.y_offsets[i]: self.y_offsets[i + 1]] for i in range(self.count)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _abi.gpu().pava_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

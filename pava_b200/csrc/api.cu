@@ -74,6 +74,52 @@ int auto_lanes_per_row(int m, int nnz) {
 
 size_t value_bytes(int precision) { return precision == PAVA_PREC_FP32C ? 4 : 8; }
 
+bool pow2_le32(int v) { return v == 1 || v == 2 || v == 4 || v == 8 || v == 16 || v == 32; }
+
+int pow2_ceil(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+// The row-group shape of a CSR handle for k right-hand sides: the handle's options where
+// given, otherwise derived from k and the mean row length.  Returns false (with a message)
+// when the given options cannot serve k.
+bool resolve_group_shape(const pava::Handle &h, int k, pava::Handle &out, std::string &why) {
+    out = h;
+    int kpl = h.cols_per_lane, kc = h.col_lanes;
+    if (kpl == 0 && kc == 0) {
+        kpl = k <= 32 ? 1 : (k <= 64 ? 2 : 4);
+        kc = pow2_ceil((k + kpl - 1) / kpl);
+    } else if (kpl == 0) {
+        kpl = (long long)kc >= k ? 1 : ((long long)kc * 2 >= k ? 2 : 4);
+    } else if (kc == 0) {
+        kc = pow2_ceil((k + kpl - 1) / kpl);
+    }
+    if (kc > 32 || (long long)kc * kpl < k) {
+        why = "col_lanes * cols_per_lane must cover k (col_lanes <= 32, cols_per_lane <= 4)";
+        return false;
+    }
+    int gl = h.lanes_per_row;
+    if (gl == 0) gl = k == 1 ? auto_lanes_per_row(h.m, h.nnz) : kc;
+    if (gl < kc) gl = h.lanes_per_row == 0 ? kc : gl;
+    if (!pow2_le32(gl) || gl < kc) {
+        why = "lanes_per_row must be a power of two <= 32 and >= col_lanes";
+        return false;
+    }
+    const int gpw = 32 / gl;
+    int tr = h.rows_per_tile ? h.rows_per_tile : 4 * gpw;
+    if (tr % gpw != 0) {
+        why = "rows_per_tile must be a multiple of 32 / lanes_per_row";
+        return false;
+    }
+    out.lanes_per_row = gl;
+    out.col_lanes = kc;
+    out.cols_per_lane = kpl;
+    out.rows_per_tile = tr;
+    return true;
+}
+
 // Builds the augmented row pointer and sizes the chunked element space (CVR, CSR5).
 pava_status plan_chunks(pava::Handle &h, const int *rp, cudaStream_t s) {
     PAVA_CUDA(dalloc(&h.arp, (size_t)h.m + 2, &h.device_bytes), "cudaMalloc(arp)");
@@ -138,17 +184,22 @@ pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double 
         if (ovf)
             return fail(PAVA_E_UNSUPPORTED_PARAMS,
                         "16-bit column offsets: a column lies more than 32767 from its chunk's first row");
-    } else {  // plain CSR: private copies
+    } else {  // plain CSR: private copies (values narrowed to float for FP32C)
         PAVA_CUDA(dalloc(&h.rp, (size_t)h.m + 1, &h.device_bytes), "cudaMalloc(rp)");
         PAVA_CUDA(dalloc(&h.ci, (size_t)h.nnz, &h.device_bytes), "cudaMalloc(ci)");
-        PAVA_CUDA(dalloc(&h.v, (size_t)h.nnz, &h.device_bytes), "cudaMalloc(v)");
+        const size_t nv = (size_t)(h.nnz ? h.nnz : 1);
+        PAVA_CUDA(cudaMalloc(&h.v, sv * nv), "cudaMalloc(v)");
+        h.device_bytes += sv * nv;
         PAVA_CUDA(cudaMemcpyAsync(h.rp, rp, sizeof(int) * ((size_t)h.m + 1),
                                   cudaMemcpyDeviceToDevice, s), "copy rp");
         if (h.nnz > 0) {
             PAVA_CUDA(cudaMemcpyAsync(h.ci, ci, sizeof(int) * (size_t)h.nnz,
                                       cudaMemcpyDeviceToDevice, s), "copy ci");
-            PAVA_CUDA(cudaMemcpyAsync(h.v, v, sizeof(double) * (size_t)h.nnz,
-                                      cudaMemcpyDeviceToDevice, s), "copy v");
+            if (h.precision == PAVA_PREC_FP32C)
+                PAVA_CUDA(pava::narrow_to_float(v, (float *)h.v, h.nnz, s), "narrow values");
+            else
+                PAVA_CUDA(cudaMemcpyAsync(h.v, v, sizeof(double) * (size_t)h.nnz,
+                                          cudaMemcpyDeviceToDevice, s), "copy v");
         }
         h.nchunks = h.m;
         h.L = 0;
@@ -157,6 +208,10 @@ pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double 
 }
 
 }  // namespace
+
+namespace pava {
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace pava
 
 extern "C" {
 
@@ -207,8 +262,8 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
         return fail(PAVA_E_UNSUPPORTED_VALUE_TYPE, "unknown precision");
     if (o.index_mode != PAVA_INDEX_I32 && o.index_mode != PAVA_INDEX_DELTA16)
         return fail(PAVA_E_UNSUPPORTED_PARAMS, "unknown index mode");
-    if (format == PAVA_FORMAT_CSR && (o.precision != PAVA_PREC_FP64 || o.index_mode != PAVA_INDEX_I32))
-        return fail(PAVA_E_UNSUPPORTED_VALUE_TYPE, "the plain CSR form is FP64 with 32-bit columns");
+    if (format == PAVA_FORMAT_CSR && o.index_mode != PAVA_INDEX_I32)
+        return fail(PAVA_E_UNSUPPORTED_PARAMS, "the plain CSR form takes 32-bit columns");
 
     pava_handle *H = new (std::nothrow) pava_handle();
     if (!H) return fail(PAVA_E_NOMEM, "host allocation failed");
@@ -236,11 +291,24 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
         }
         h.L = 32LL * h.sigma * h.G;
     } else {
-        h.lanes_per_row = o.lanes_per_row ? o.lanes_per_row : auto_lanes_per_row(h.m, h.nnz);
-        const int V = h.lanes_per_row;
-        if (!(V == 1 || V == 2 || V == 4 || V == 8 || V == 16 || V == 32)) {
+        // 0 = derive per call (resolve_group_shape)
+        h.lanes_per_row = o.lanes_per_row;
+        h.col_lanes = o.col_lanes;
+        h.cols_per_lane = o.cols_per_lane;
+        h.rows_per_tile = o.rows_per_tile;
+        std::string why;
+        pava::Handle probe;
+        if ((o.lanes_per_row && !pow2_le32(o.lanes_per_row)) ||
+            (o.col_lanes && !pow2_le32(o.col_lanes)) ||
+            !(o.cols_per_lane == 0 || o.cols_per_lane == 1 || o.cols_per_lane == 2 ||
+              o.cols_per_lane == 4) ||
+            o.rows_per_tile < 0 || o.rows_per_tile > (1 << 20) ||
+            !resolve_group_shape(h, 1, probe, why)) {
             delete H;
-            return fail(PAVA_E_UNSUPPORTED_PARAMS, "lanes_per_row must be a power of two <= 32");
+            return fail(PAVA_E_UNSUPPORTED_PARAMS,
+                        why.empty() ? "CSR group shape: lanes_per_row / col_lanes powers of two "
+                                      "<= 32, cols_per_lane 1, 2 or 4"
+                                    : why);
         }
     }
     cudaStream_t s = (cudaStream_t)stream;
@@ -330,9 +398,32 @@ pava_status pava_spmv_stage(pava_handle *H, const void *x, void *y, void *stream
         if (main_k) e = pava::csr5_spmv(h, x, y, s);
         if (e == cudaSuccess && fix_k) e = pava::carry_fixup(h, y, s);
     } else {
-        if (main_k) e = pava::csr_spmv(h, x, y, s);
+        if (main_k) {
+            pava::Handle g;
+            std::string why;
+            if (!resolve_group_shape(h, 1, g, why)) return fail(PAVA_E_UNSUPPORTED_PARAMS, why);
+            e = pava::csr_spmv(g, x, y, s);
+        }
     }
     if (e != cudaSuccess) return fail_cuda(e, "spmv launch");
+    return PAVA_SUCCESS;
+}
+
+pava_status pava_spmm(pava_handle *H, int k, const void *X, long long ldx, void *Y,
+                      long long ldy, void *stream) {
+    if (!H) return fail(PAVA_E_INVALID_ARG, "handle is NULL");
+    pava::Handle &h = H->h;
+    if (h.format != PAVA_FORMAT_CSR)
+        return fail(PAVA_E_UNKNOWN_FORMAT, "pava_spmm needs a CSR handle");
+    if (k < 1 || k > 128) return fail(PAVA_E_INVALID_ARG, "k must be in [1, 128]");
+    if (ldx < k || ldy < k) return fail(PAVA_E_INVALID_ARG, "ldx and ldy must be >= k");
+    if (h.m == 0) return PAVA_SUCCESS;
+    if (!X || !Y) return fail(PAVA_E_INVALID_ARG, "X or Y is NULL");
+    pava::Handle g;
+    std::string why;
+    if (!resolve_group_shape(h, k, g, why)) return fail(PAVA_E_UNSUPPORTED_PARAMS, why);
+    cudaError_t e = pava::csr_spmm(g, X, ldx, Y, ldy, k, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "spmm launch");
     return PAVA_SUCCESS;
 }
 

@@ -1,5 +1,5 @@
-// Support kernels: CSR validation, the augmented row pointer, the deterministic carry fixup
-// shared by the CVR and CSR5 forms, and the plain-CSR kernel (baseline and in-GPU checker).
+// Support kernels: CSR validation, the augmented row pointer and the deterministic carry fixup
+// shared by the CVR and CSR5 forms.
 
 #include <cub/cub.cuh>
 
@@ -68,35 +68,6 @@ __global__ void carry_fixup_kernel(const char *__restrict__ meta, size_t stride,
     }
 }
 
-// Plain CSR, V lanes per row, FP64: sum over the row in lane-strided order, then a fixed
-// butterfly over the V lanes.
-template <int V>
-__global__ void __launch_bounds__(256)
-csr_vector_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
-                  const double *__restrict__ v, const double *__restrict__ x,
-                  double *__restrict__ y, int m) {
-    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long row = gt / V;
-    const int sub = (int)(gt % V);
-    const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
-    double s = 0.0;
-    if (row < m) {
-        const int a = rp[row], b = rp[row + 1];
-        for (int j = a + sub; j < b; j += V) {
-            double val;
-            int col;
-            asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;"
-                         : "=d"(val) : "l"(v + j), "l"(pf));
-            asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
-                         : "=r"(col) : "l"(ci + j), "l"(pf));
-            s = fma(val, ld_x(x + col, pl), s);
-        }
-    }
-#pragma unroll
-    for (int d = V / 2; d > 0; d >>= 1) s += __shfl_xor_sync(FULL, s, d);
-    if (row < m && sub == 0) y[row] = s;
-}
-
 }  // namespace
 
 cudaError_t launch_validate(const int *rp, const int *ci, int m, int n, int nnz, int *d_err,
@@ -144,24 +115,6 @@ cudaError_t carry_fixup(const Handle &h, void *y, cudaStream_t s) {
     carry_fixup_kernel<<<(unsigned)blocks, 256, 0, s>>>((const char *)h.meta, h.meta_stride,
                                                         h.arp, h.L, h.carry_head, h.carry_tail,
                                                         (double *)y, h.nchunks, h.m);
-    return cudaGetLastError();
-}
-
-cudaError_t csr_spmv(const Handle &h, const void *x, void *y, cudaStream_t s) {
-    if (h.m <= 0) return cudaSuccess;
-    const long long threads = (long long)h.m * h.lanes_per_row;
-    const unsigned blocks = (unsigned)((threads + 255) / 256);
-    const double *xd = (const double *)x;
-    double *yd = (double *)y;
-    switch (h.lanes_per_row) {
-        case 1: csr_vector_kernel<1><<<blocks, 256, 0, s>>>(h.rp, h.ci, h.v, xd, yd, h.m); break;
-        case 2: csr_vector_kernel<2><<<blocks, 256, 0, s>>>(h.rp, h.ci, h.v, xd, yd, h.m); break;
-        case 4: csr_vector_kernel<4><<<blocks, 256, 0, s>>>(h.rp, h.ci, h.v, xd, yd, h.m); break;
-        case 8: csr_vector_kernel<8><<<blocks, 256, 0, s>>>(h.rp, h.ci, h.v, xd, yd, h.m); break;
-        case 16: csr_vector_kernel<16><<<blocks, 256, 0, s>>>(h.rp, h.ci, h.v, xd, yd, h.m); break;
-        case 32: csr_vector_kernel<32><<<blocks, 256, 0, s>>>(h.rp, h.ci, h.v, xd, yd, h.m); break;
-        default: return cudaErrorInvalidValue;
-    }
     return cudaGetLastError();
 }
 

@@ -4,6 +4,8 @@
 #include <stdint.h>
 #include <stddef.h>
 
+#include <string>
+
 #include "../../include/pava_gpu.h"
 #include "pava_common.cuh"
 
@@ -36,7 +38,10 @@ struct Handle {
     int S = 0;               // CVR: steps per chunk
     int sigma = 0, G = 0;    // CSR5: elements per lane per tile, tiles per chunk
     long long ntiles = 0;
-    int lanes_per_row = 0;   // plain CSR
+    int lanes_per_row = 0;   // plain CSR: lanes per row group (GL)
+    int col_lanes = 1;       //   lanes across the right-hand sides (KC)
+    int cols_per_lane = 1;   //   right-hand sides per lane (KPL)
+    int rows_per_tile = 0;   //   rows per warp tile of the persistent launch (TR)
     int device = 0, sm_count = 0;
 
     int *arp = nullptr;            // augmented row pointer, m + 2 entries (row m = padding)
@@ -49,11 +54,14 @@ struct Handle {
     double *carry_head = nullptr;  // per-chunk partial of a first row shared with the left
     double *carry_tail = nullptr;  // per-chunk partial of a last row shared with the right
     int *rp = nullptr, *ci = nullptr;  // plain CSR form
-    double *v = nullptr;
+    void *v = nullptr;                 //   values: double, or float for FP32C
 
     double convert_ms = 0.0;
     size_t device_bytes = 0;
 };
+
+// Sets the message pava_last_error() returns on this thread.
+void set_last_error(const std::string &msg);
 
 // Kernel launchers (stream-ordered; return cudaGetLastError()).
 cudaError_t launch_validate(const int *rp, const int *ci, int m, int n, int nnz, int *d_err,
@@ -72,6 +80,11 @@ cudaError_t csr5_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
 
 cudaError_t carry_fixup(const Handle &h, void *y, cudaStream_t s);
 
+// Plain CSR row-group kernel: y = A x, and Y = A X with X row-major n x k (leading
+// dimensions ldx, ldy in elements).
 cudaError_t csr_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
+cudaError_t csr_spmm(const Handle &h, const void *X, long long ldx, void *Y, long long ldy,
+                     int k, cudaStream_t s);
+cudaError_t narrow_to_float(const double *src, float *dst, long long n, cudaStream_t s);
 
 }  // namespace pava

@@ -1,0 +1,238 @@
+"""Multi-RHS products, batches of independent matrices, graph replay and the autotuner,
+through the C ABI, against the CPU oracle (long-double CSR sums).
+
+Bounds: FP64 forms 1e-12 relative per row and right-hand side (cancellation-aware
+denominator); FP32C forms 1e-9 on FP32-representable inputs."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pava_b200 import _abi
+from pava_b200 import matrices as M
+from pava_b200.api import Batch, SpMatrix, autotune
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+TOL32 = 1e-9
+
+
+def _check_cols(A, X, Y, tol):
+    for j in range(X.shape[1]):
+        yr, ab = O.csr_ref(A.rp, A.ci, A.v, np.ascontiguousarray(X[:, j]))
+        bad, mx, _ = O.rel_error(np.ascontiguousarray(Y[:, j]), yr, ab, tol)
+        assert bad == 0, (j, mx)
+
+
+def _x(torch, n, k, seed, fp32=False):
+    X = M.uniform(n * k, seed=seed, fp32=fp32).reshape(n, k)
+    return X, torch.from_numpy(X).to("cuda", torch.float32 if fp32 else torch.float64)
+
+
+SHAPES = [  # (k, lanes_per_row, col_lanes, cols_per_lane, rows_per_tile)
+    (1, 0, 0, 0, 0), (1, 4, 1, 1, 64), (1, 32, 1, 1, 1), (2, 8, 2, 1, 0), (8, 8, 8, 1, 4),
+    (8, 32, 8, 1, 0), (8, 16, 4, 2, 0), (13, 16, 16, 1, 2), (32, 32, 32, 1, 0),
+    (32, 32, 16, 2, 3), (32, 16, 8, 4, 0), (64, 32, 32, 2, 0), (100, 32, 32, 4, 1),
+]
+
+
+@pytest.mark.parametrize("k,gl,kc,kpl,tr", SHAPES, ids=[f"k{s[0]}_g{s[1]}_c{s[2]}_p{s[3]}_t{s[4]}" for s in SHAPES])
+def test_spmm_banded_shapes(cuda, k, gl, kc, kpl, tr):
+    torch = cuda
+    A = M.banded(20_000, 64, 24, seed=11)
+    X, Xd = _x(torch, A.n, k, seed=12)
+    mat = SpMatrix(A, "csr", lanes_per_row=gl, col_lanes=kc, cols_per_lane=kpl, rows_per_tile=tr)
+    Y = mat.spmm(Xd).cpu().numpy()
+    _check_cols(A, X, Y, TOL)
+
+
+def test_spmm_irregular_rows_and_strides(cuda):
+    torch = cuda
+    A = M.powerlaw(30_000, mean=16.0, cap=5_000, p_empty=0.05, seed=13)
+    X, Xd = _x(torch, A.n, 24, seed=14)
+    # X and Y as column slices of wider row-major buffers (ldx, ldy > k)
+    Xw = torch.zeros((A.n, 40), dtype=torch.float64, device="cuda")
+    Xw[:, 3:27] = Xd
+    Yw = torch.full((A.m, 33), float("nan"), dtype=torch.float64, device="cuda")
+    mat = SpMatrix(A, "csr", lanes_per_row=32, col_lanes=8, cols_per_lane=4)
+    mat.spmm(Xw[:, 3:27], Yw[:, 5:29])
+    Y = Yw[:, 5:29].cpu().numpy()
+    _check_cols(A, X, Y, TOL)
+    assert torch.isnan(Yw[:, :5]).all() and torch.isnan(Yw[:, 29:]).all()
+
+
+def test_spmm_k1_equals_spmv(cuda):
+    torch = cuda
+    A = M.random_csr(50_000, mean=12.0, seed=15)
+    x = M.uniform(A.n, seed=16)
+    mat = SpMatrix(A, "csr", lanes_per_row=4)
+    y1 = mat.spmv(torch.from_numpy(x).cuda()).cpu().numpy()
+    y2 = mat.spmm(torch.from_numpy(x).cuda().reshape(-1, 1)).cpu().numpy()[:, 0]
+    assert np.array_equal(y1, y2)
+
+
+def test_spmm_fp32c(cuda):
+    torch = cuda
+    A = M.stencil27(24, seed=17)
+    X, Xd = _x(torch, A.n, 8, seed=18, fp32=True)
+    mat = SpMatrix(A, "csr", precision=_abi.PREC_FP32C, lanes_per_row=8, col_lanes=8)
+    Y = mat.spmm(Xd).cpu().numpy()
+    _check_cols(A, X, Y, TOL32)
+
+
+@pytest.mark.parametrize("kw", [dict(lanes_per_row=3), dict(col_lanes=64),
+                                dict(cols_per_lane=3), dict(lanes_per_row=4, col_lanes=8),
+                                dict(lanes_per_row=4, rows_per_tile=3)],
+                         ids=["gl3", "kc64", "kpl3", "kc_gt_gl", "tr_not_multiple"])
+def test_csr_shape_rejected(cuda, kw):
+    A = M.random_csr(1000, seed=19)
+    with pytest.raises(_abi.PavaError) as e:
+        SpMatrix(A, "csr", **kw)
+    assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
+
+
+def test_spmm_k_not_covered(cuda):
+    torch = cuda
+    A = M.random_csr(1000, seed=20)
+    mat = SpMatrix(A, "csr", col_lanes=4, cols_per_lane=2)
+    Xd = torch.zeros((A.n, 9), dtype=torch.float64, device="cuda")
+    with pytest.raises(_abi.PavaError) as e:
+        mat.spmm(Xd)
+    assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
+
+
+# ---- batches ------------------------------------------------------------------------------
+
+def _batch_mats(count, seed, lo=64, hi=6000):
+    rng = np.random.default_rng(seed)
+    mats = []
+    for i in range(count):
+        m = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        mats.append(M.random_csr(m, mean=12.0, seed=seed * 1000 + i))
+    # uneven extras: an all-empty matrix, one with empty rows, a rectangular one, 1 x 1
+    mats.append(M.from_arrays(40, 40, np.zeros(41, np.int32), [], []))
+    mats.append(M.powerlaw(3000, mean=4.0, p_empty=0.3, seed=seed + 1))
+    mats.append(M.random_csr(700, n=1900, mean=9.0, seed=seed + 2))
+    mats.append(M.from_arrays(1, 1, [0, 1], [0], [2.5]))
+    return mats
+
+
+def _check_batch(b, mats, xs, y, tol):
+    for i, A in enumerate(mats):
+        yi = y[b.y_offsets[i]: b.y_offsets[i + 1]]
+        yr, ab = O.csr_ref(A.rp, A.ci, A.v, xs[i])
+        bad, mx, _ = O.rel_error(yi, yr, ab, tol)
+        assert bad == 0, (i, mx)
+
+
+BATCH_FORMS = [("csr", dict(lanes_per_row=4)), ("csr", dict(lanes_per_row=16, rows_per_tile=32)),
+               ("cvr", dict(steps=64)), ("csr5", dict(sigma=16)), ("auto", {})]
+
+
+@pytest.mark.parametrize("fmt,kw", BATCH_FORMS, ids=["csr4", "csr16", "cvr", "csr5", "auto"])
+def test_batch_matches_each_matrix(cuda, fmt, kw):
+    torch = cuda
+    mats = _batch_mats(60, seed=21)
+    b = Batch(mats, fmt, **kw)
+    assert b.count == len(mats) and b.m == sum(A.m for A in mats)
+    xs = [M.uniform(A.n, seed=100 + i) for i, A in enumerate(mats)]
+    x = torch.from_numpy(np.concatenate(xs)).cuda()
+    y = b.spmv(x).cpu().numpy()
+    _check_batch(b, mats, xs, y, TOL)
+    if fmt == "auto":
+        f, o = b.chosen()
+        assert f in ("csr", "cvr", "csr5")
+
+
+def test_batch_graph_replay_bitwise(cuda):
+    torch = cuda
+    mats = _batch_mats(40, seed=22)
+    b = Batch(mats, "csr", lanes_per_row=4)
+    xs = [M.uniform(A.n, seed=200 + i) for i, A in enumerate(mats)]
+    x = torch.from_numpy(np.concatenate(xs)).cuda()
+    y_direct = b.spmv(x).cpu().numpy()
+    y = torch.full((b.m,), float("nan"), dtype=torch.float64, device="cuda")
+    b.capture(x, y)
+    for _ in range(3):
+        y.fill_(float("nan"))
+        b.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(y.cpu().numpy(), y_direct)
+    # the graph reads x at replay time: new x values, same buffer
+    xs2 = [M.uniform(A.n, seed=300 + i) for i, A in enumerate(mats)]
+    x.copy_(torch.from_numpy(np.concatenate(xs2)))
+    b.replay()
+    torch.cuda.synchronize()
+    _check_batch(b, mats, xs2, y.cpu().numpy(), TOL)
+
+
+def test_batch_fp32c(cuda):
+    torch = cuda
+    mats = [M.stencil27(g, seed=23 + g) for g in (6, 9, 13)] + _batch_mats(10, seed=24)
+    for A in mats:
+        A.v = A.v.astype(np.float32).astype(np.float64)
+    xs = [M.uniform(A.n, seed=400 + i, fp32=True) for i, A in enumerate(mats)]
+    for fmt, kw in [("csr", dict(lanes_per_row=8)), ("csr5", dict(sigma=32))]:
+        b = Batch(mats, fmt, precision=_abi.PREC_FP32C, **kw)
+        x = torch.from_numpy(np.concatenate(xs)).to("cuda", torch.float32)
+        y = b.spmv(x).cpu().numpy()
+        _check_batch(b, mats, xs, y, TOL32)
+
+
+def test_batch_rejects_bad_matrix(cuda):
+    mats = _batch_mats(5, seed=25)
+    bad = M.random_csr(100, seed=26)
+    bad.ci = bad.ci.copy()
+    bad.ci[7] = 100  # column == n
+    with pytest.raises(_abi.PavaError) as e:
+        Batch(mats + [bad], "csr")
+    assert e.value.status == _abi.E_INVALID_CSR
+    norows = M.from_arrays(0, 5, [0], [], [])
+    norows.rp = np.array([3], np.int32)  # claims 3 nonzeros with no rows
+    norows.ci = np.zeros(3, np.int32)
+    norows.v = np.ones(3)
+    with pytest.raises(_abi.PavaError) as e:
+        Batch(mats + [norows], "csr")
+    assert e.value.status == _abi.E_INVALID_CSR
+
+
+# ---- autotuner ----------------------------------------------------------------------------
+
+def test_autotune_k1_runs_every_candidate(cuda):
+    A = M.powerlaw(100_000, mean=16.0, cap=20_000, seed=27)
+    ents, best = autotune(A, k=1, reps=3)
+    forms = {e["format"] for e in ents}
+    assert {"cvr", "csr5", "csr"} <= forms
+    assert all(e["ms"] > 0 and e["status"] == 0 for e in ents)
+    assert ents[best]["ms"] == min(e["ms"] for e in ents)
+    # the winner computes the right product
+    torch = cuda
+    x = M.uniform(A.n, seed=28)
+    e = ents[best]
+    opts = {k: v for k, v in e["opts"].items() if v and k != "precision"}
+    y = SpMatrix(A, e["format"], **opts).spmv(torch.from_numpy(x).cuda()).cpu().numpy()
+    yr, ab = O.csr_ref(A.rp, A.ci, A.v, x)
+    assert O.rel_error(y, yr, ab, TOL)[0] == 0
+
+
+@pytest.mark.parametrize("k", [8, 32])
+def test_autotune_spmm(cuda, k):
+    A = M.banded(50_000, 64, 24, seed=29)
+    ents, best = autotune(A, k=k, reps=3)
+    assert all(e["format"] == "csr" for e in ents)
+    assert all(e["opts"]["col_lanes"] * e["opts"]["cols_per_lane"] >= k for e in ents)
+    assert ents[best]["ms"] > 0
+
+
+# ---- the batching configuration at full size ----------------------------------------------
+
+def test_config4_banded_full(cuda):
+    """1,048,576-row banded matrix (half-bandwidth 64, 24 per row), k = 1, 8, 32."""
+    torch = cuda
+    A = M.banded(1_048_576, 64, 24, seed=3)
+    for k in (1, 8, 32):
+        X, Xd = _x(torch, A.n, k, seed=30 + k)
+        Y = SpMatrix(A, "csr").spmm(Xd).cpu().numpy()
+        for j in sorted({0, k // 2, k - 1}):
+            yr, ab = O.csr_ref(A.rp, A.ci, A.v, np.ascontiguousarray(X[:, j]))
+            assert O.rel_error(np.ascontiguousarray(Y[:, j]), yr, ab, TOL)[0] == 0
