@@ -199,6 +199,89 @@ typedef struct pava_tune_entry {
 pava_status pava_autotune(const pava_csr *A, int k, int precision, int reps,
                           pava_tune_entry *entries, int max_entries, int *n_entries, int *best);
 
+/* ---- Device-side generators --------------------------------------------------------
+ * Seeded synthetic matrices built on the GPU (one thread per row for the lengths, one per
+ * nonzero for columns and values), for workloads too large to build on the host.  Columns
+ * are sorted and distinct per row, values N(0,1).  No counterpart in the reference (it
+ * reads .mtx files, utils/basicMatrix.cpp:63-253).  Families and parameters:
+ *   STENCIL   p0 = dimensions (2 or 3), p1 = points (5/9 in 2-D, 7/27 in 3-D); m is rounded
+ *             down to a g^d grid
+ *   BANDED    p0 = half-bandwidth, p1 = nonzeros per row (clipped to the band)
+ *   POWERLAW  p0 = mean row length, p1 = lognormal sigma, p2 = cap, p3 = share of empty rows
+ *   BLOCKDIAG p0 = smallest block, p1 = largest block (dense square blocks)
+ * n = 0 means n = m.  The CSR is allocated on the device; free it with
+ * pava_free_device_csr. */
+typedef enum pava_gen_family {
+    PAVA_GEN_STENCIL = 0,
+    PAVA_GEN_BANDED = 1,
+    PAVA_GEN_POWERLAW = 2,
+    PAVA_GEN_BLOCKDIAG = 3
+} pava_gen_family;
+typedef struct pava_gen_params {
+    int family;
+    int m, n;
+    double p0, p1, p2, p3;
+} pava_gen_params;
+pava_status pava_gen_device(const pava_gen_params *p, uint64_t seed, void *stream,
+                            pava_csr *out);
+pava_status pava_free_device_csr(pava_csr *A);
+
+/* ---- Learned form selector ----------------------------------------------------------
+ * No counterpart in the reference (which runs every format it is asked for).  Six engine
+ * variants -- the form and its tile parameter:
+ *   0 CVR steps 64    1 CVR steps 128    2 CSR5 sigma 16    3 CSR5 sigma 32
+ *   4 CSR 4 lanes per row                5 CSR 32 lanes per row
+ * A matrix is described by 12 structural features (pava_features), an MLP 12-64-64-6
+ * predicts the log-time of each variant, and the smallest prediction wins.  The network is
+ * trained on the GPU by the library's own forward / backward / Adam kernels on timings that
+ * pava_time_variants measures; exhaustive timing is both the fallback and the yardstick of
+ * the selector's regret. */
+#define PAVA_NVARIANTS 6
+#define PAVA_MLP_IN 12
+#define PAVA_MLP_HIDDEN 64
+#define PAVA_MLP_OUT 6
+#define PAVA_MLP_NPARAM 5382
+/* Variant v's format and options (options zeroed except the variant's tile parameter). */
+pava_status pava_variant(int v, int *format, pava_opts *opts);
+/* Structural features of a device CSR (sorted columns), 12 floats:
+ *   0 log10 m   1 log10 nnz   2 log10 mean row length   3 row-length std / mean
+ *   4 log10 max / mean row length   5 share of empty rows   6 share of nonzeros in rows
+ *   longer than 64   7 share of rows with 1..4 nonzeros   8 log10(mean |col - row| / n + 1e-7)
+ *   9 share of nonzeros within 64 of the diagonal   10 distinct 128-byte x lines per
+ *   nonzero   11 log10(mean row span / n + 1e-7).  Integer accumulation: same bits each run. */
+pava_status pava_features(const pava_csr *A, float *out12, void *stream);
+/* Converts A into each variant and times its SpMV (one warm-up, median of `reps` CUDA-event
+ * timings, x and y on the device); ms[v] < 0 when variant v failed; *best = fastest. */
+pava_status pava_time_variants(const pava_csr *A, int reps, double *ms, int *best);
+typedef struct pava_mlp pava_mlp;
+/* A network with He-uniform weights from `seed`, zero biases, identity normalisation. */
+pava_status pava_mlp_create(uint64_t seed, pava_mlp **out);
+/* Parameters (PAVA_MLP_NPARAM floats: W1[64][12] b1 W2[64][64] b2 W3[6][64] b3) and the
+ * feature normalisation (x - mean) / std applied to every batch; any pointer may be NULL.
+ * Setting parameters resets the Adam state. */
+pava_status pava_mlp_get_params(const pava_mlp *m, float *params, float *mean12, float *std12);
+pava_status pava_mlp_set_params(pava_mlp *m, const float *params, const float *mean12,
+                                const float *std12);
+/* Uploads a batch: B x 12 raw features, optional B x 6 targets and 0/1 mask (NULL mask = all
+ * ones).  The loss is the masked mean squared error. */
+pava_status pava_mlp_set_batch(pava_mlp *m, int B, const float *X, const float *T,
+                               const float *mask);
+/* Outputs for the current batch (B x 6, host). */
+pava_status pava_mlp_forward(pava_mlp *m, float *Y);
+/* Gradient of the loss w.r.t. the parameters (PAVA_MLP_NPARAM floats, host) and the loss. */
+pava_status pava_mlp_gradient(pava_mlp *m, float *grad, float *loss);
+/* `epochs` full-batch Adam steps (beta 0.9 / 0.999, eps 1e-8) on the current batch;
+ * loss_hist (may be NULL) receives the loss before each step. */
+pava_status pava_mlp_train(pava_mlp *m, int epochs, float lr, float *loss_hist);
+pava_status pava_mlp_destroy(pava_mlp *m);
+/* The variant the network predicts fastest for a device CSR (and the 6 predictions).  Uses
+ * the network's batch slot (a 1-sample batch replaces the current one). */
+pava_status pava_select(pava_mlp *m, const pava_csr *A, int *variant, float *pred6);
+/* pava_create with the selected variant: by the network when m != NULL and A is on the
+ * device, otherwise by timing all six (the exhaustive fallback). */
+pava_status pava_create_selected(const pava_csr *A, pava_mlp *m, void *stream,
+                                 pava_handle **out, int *variant);
+
 /* Drop-ins for the reference's engine entry points, same signatures and meaning:
  * conduct_cvr (cvr/cvr.h:1953) and conduct_csr5 (csr5/csr5.h:72-74).  Each copies the CSR to
  * the device, converts (timed as the convert column), runs one SpMV into refOut / y (the

@@ -60,6 +60,15 @@ class PavaTuneEntry(ctypes.Structure):
     _fields_ = [("format", c_int), ("opts", PavaOpts), ("ms", c_dbl), ("status", c_int)]
 
 
+class PavaGenParams(ctypes.Structure):
+    _fields_ = [("family", c_int), ("m", c_int), ("n", c_int), ("p0", c_dbl), ("p1", c_dbl),
+                ("p2", c_dbl), ("p3", c_dbl)]
+
+
+GEN_STENCIL, GEN_BANDED, GEN_POWERLAW, GEN_BLOCKDIAG = 0, 1, 2, 3
+NVARIANTS, MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_NPARAM = 6, 12, 64, 6, 5382
+
+
 class PavaError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"pava status {status}: {msg}")
@@ -93,6 +102,25 @@ GPU_SYMBOLS = [
     ("pava_autotune", c_int, [ctypes.POINTER(PavaCsr), c_int, c_int, c_int,
                               ctypes.POINTER(PavaTuneEntry), c_int, ctypes.POINTER(c_int),
                               ctypes.POINTER(c_int)]),
+    ("pava_gen_device", c_int, [ctypes.POINTER(PavaGenParams), c_u64, c_void_p,
+                                ctypes.POINTER(PavaCsr)]),
+    ("pava_free_device_csr", c_int, [ctypes.POINTER(PavaCsr)]),
+    ("pava_features", c_int, [ctypes.POINTER(PavaCsr), c_void_p, c_void_p]),
+    ("pava_variant", c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(PavaOpts)]),
+    ("pava_time_variants", c_int, [ctypes.POINTER(PavaCsr), c_int, c_void_p,
+                                   ctypes.POINTER(c_int)]),
+    ("pava_mlp_create", c_int, [c_u64, ctypes.POINTER(c_void_p)]),
+    ("pava_mlp_get_params", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("pava_mlp_set_params", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("pava_mlp_set_batch", c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    ("pava_mlp_forward", c_int, [c_void_p, c_void_p]),
+    ("pava_mlp_gradient", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("pava_mlp_train", c_int, [c_void_p, c_int, ctypes.c_float, c_void_p]),
+    ("pava_mlp_destroy", c_int, [c_void_p]),
+    ("pava_select", c_int, [c_void_p, ctypes.POINTER(PavaCsr), ctypes.POINTER(c_int),
+                            c_void_p]),
+    ("pava_create_selected", c_int, [ctypes.POINTER(PavaCsr), c_void_p, c_void_p,
+                                     ctypes.POINTER(c_void_p), ctypes.POINTER(c_int)]),
     ("conduct_cvr_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_int, c_char_p, c_int]),
     ("conduct_csr5_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -1,0 +1,76 @@
+"""CPU side of the learned selector: the committed training set and the CPU restatement of
+the network used as the checker of the GPU kernels (no GPU needed)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import selector_ref as R
+from pava_b200 import selector as S
+
+DATA = os.path.join(os.path.dirname(__file__), "golden", "selector_timings.npz")
+
+
+def test_training_set_file():
+    if not os.path.exists(DATA):
+        pytest.fail("tests/golden/selector_timings.npz is missing (python -m pava_b200.selector generate)")
+    d = np.load(DATA)
+    n = int(d["n_train"]) + int(d["n_test"])
+    assert (int(d["n_train"]), int(d["n_test"])) == (2000, 200)
+    assert d["features"].shape == (n, 12) and d["times_ms"].shape == (n, 6)
+    assert np.isfinite(d["features"]).all()
+    assert (d["times_ms"] > 0).mean() > 0.99          # nearly every variant ran
+    assert np.all(np.bincount(d["family"], minlength=4) == n // 4)
+    assert d["rows"].min() >= 1e4 - 1 and d["rows"].max() <= 1e7
+    assert d["nnz"].min() >= 5e4 and d["nnz"].max() <= 1.1e8
+    # matrix i's spec is a pure function of i
+    for i in (0, 1, 2, 3, 1234):
+        assert S.spec(i) == S.spec(i)
+        assert S.spec(i)["family"] == d["family"][i]
+
+
+def test_specs_cover_the_ranges():
+    rows, fam = [], []
+    for i in range(400):
+        sp = S.spec(i)
+        rows.append(sp["m"])
+        fam.append(sp["family"])
+    rows = np.array(rows)
+    assert rows.min() >= 1e4 and rows.max() <= 1e7
+    assert np.log10(rows).std() > 0.5
+    assert np.all(np.bincount(fam) == 100)
+
+
+def test_cpu_gradient_against_finite_differences():
+    rng = np.random.default_rng(1)
+    P = rng.normal(scale=0.3, size=R.NP)
+    X = rng.normal(size=(50, 12))
+    T = rng.normal(size=(50, 6))
+    mask = (rng.uniform(size=(50, 6)) > 0.2).astype(float)
+    loss, g = R.mlp_loss_grad(P, X, T, mask)
+    for p in rng.choice(R.NP, 40, replace=False):
+        h = 1e-6
+        Pp, Pm = P.copy(), P.copy()
+        Pp[p] += h
+        Pm[p] -= h
+        fd = (R.mlp_loss_grad(Pp, X, T, mask)[0] - R.mlp_loss_grad(Pm, X, T, mask)[0]) / (2 * h)
+        assert abs(fd - g[p]) <= 1e-7 + 1e-5 * abs(g[p])
+
+
+def test_regret_definition():
+    t = np.array([[1.0, 2.0, 1.5, 4.0, 1.1, 3.0], [2.0, 1.0, -1.0, 1.0, 5.0, 2.0]])
+    r = S.regret(t, np.array([4, 2]))
+    assert np.isclose(r[0], 0.1) and np.isinf(r[1])   # a failed variant is never acceptable
+    assert np.array_equal(S.regret(t, np.array([0, 1])), [0.0, 0.0])
+
+
+def test_cpu_features_small():
+    # 3 x 4: row 0 = cols {0, 1}, row 1 empty, row 2 = cols {1, 3, 20}
+    rp = np.array([0, 2, 2, 5])
+    ci = np.array([0, 1, 1, 3, 20])
+    f = R.features(rp, ci, 40)
+    assert np.isclose(f[0], np.log10(3)) and np.isclose(f[1], np.log10(5))
+    assert np.isclose(f[5], 1 / 3)                     # one empty row
+    assert np.isclose(f[7], 2 / 3)                     # two rows with 1..4 nonzeros
+    assert np.isclose(f[10], (1 + 2) / 5)              # x lines: row 0 one, row 2 two
+    assert np.isclose(f[9], 1.0)                       # all within 64 of the diagonal
