@@ -1,7 +1,7 @@
 """The learned form selector: training set generation, GPU training, selection and regret.
 
-    python -m pava_b200.selector generate --out tests/golden/selector_timings.npz
-    python -m pava_b200.selector evaluate --data tests/golden/selector_timings.npz
+    python -m pava_b200.selector generate --out tests/golden/selector/selector_timings.npz
+    python -m pava_b200.selector evaluate --data tests/golden/selector/selector_timings.npz
 
 Training set: 2,000 training and 200 held-out matrices; matrix i is drawn from a generator
 seeded with i.  Families (in turn): stencil (2-D 5/9-point, 3-D 7/27-point), banded-random,
@@ -256,8 +256,8 @@ def train_selector(data, epochs=3000, lr=3e-3, seed=0):
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("cmd", choices=["generate", "evaluate"])
-    p.add_argument("--out", default="tests/golden/selector_timings.npz")
-    p.add_argument("--data", default="tests/golden/selector_timings.npz")
+    p.add_argument("--out", default="tests/golden/selector/selector_timings.npz")
+    p.add_argument("--data", default="tests/golden/selector/selector_timings.npz")
     p.add_argument("--train", type=int, default=N_TRAIN)
     p.add_argument("--test", type=int, default=N_TEST)
     p.add_argument("--reps", type=int, default=5)

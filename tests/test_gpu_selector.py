@@ -16,7 +16,7 @@ from pava_b200.api import SpMatrix
 
 pytestmark = pytest.mark.gpu
 
-DATA = os.path.join(os.path.dirname(__file__), "golden", "selector_timings.npz")
+DATA = os.path.join(os.path.dirname(__file__), "golden", "selector", "selector_timings.npz")
 
 
 class _DevArray:
@@ -209,7 +209,7 @@ def test_time_variants_all_run(cuda):
 def test_selector_regret_on_training_set(cuda):
     """Trained on the committed timings of 2,000 matrices, judged on the 200 held-out ones:
     mean regret vs exhaustive timing <= 10 %, and below the best single fixed variant's."""
-    assert os.path.exists(DATA), "tests/golden/selector_timings.npz is missing"
+    assert os.path.exists(DATA), "tests/golden/selector/selector_timings.npz is missing"
     d = dict(np.load(DATA))
     assert int(d["n_train"]) == 2000 and int(d["n_test"]) == 200
     _, rep = S.train_selector(d, epochs=3000, lr=3e-3, seed=0)

@@ -8,12 +8,12 @@ import pytest
 from oracle import selector_ref as R
 from pava_b200 import selector as S
 
-DATA = os.path.join(os.path.dirname(__file__), "golden", "selector_timings.npz")
+DATA = os.path.join(os.path.dirname(__file__), "golden", "selector", "selector_timings.npz")
 
 
 def test_training_set_file():
     if not os.path.exists(DATA):
-        pytest.fail("tests/golden/selector_timings.npz is missing (python -m pava_b200.selector generate)")
+        pytest.fail("tests/golden/selector/selector_timings.npz is missing (python -m pava_b200.selector generate)")
     d = np.load(DATA)
     n = int(d["n_train"]) + int(d["n_test"])
     assert (int(d["n_train"]), int(d["n_test"])) == (2000, 200)
