@@ -40,14 +40,18 @@ __device__ __forceinline__ int ld_col(const int *p, uint64_t pol) {
 }
 
 constexpr int GROUP_THREADS = 256;
-constexpr int GROUP_MINB = 4;
+// resident blocks per SM: more warps in flight for the narrow shapes
+template <int KPL> constexpr int group_minb() { return KPL == 1 ? 6 : (KPL == 2 ? 5 : 4); }
+// elements in flight per lane
+template <int KPL> constexpr int group_unroll() { return KPL == 1 ? 4 : (KPL == 2 ? 2 : 1); }
 
 template <int KPL, typename VT>
-__global__ void __launch_bounds__(GROUP_THREADS, GROUP_MINB)
+__global__ void __launch_bounds__(GROUP_THREADS, group_minb<KPL>())
 csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                  const VT *__restrict__ v, const VT *__restrict__ X, long long ldx,
                  double *__restrict__ Y, long long ldy, int m, int k, int gl_shift,
                  int kc_shift, int tile_rows) {
+    constexpr int U = group_unroll<KPL>();
     const int lane = threadIdx.x & 31;
     const int gl = 1 << gl_shift, kc = 1 << kc_shift;
     const int grp = lane >> gl_shift;          // group within the warp
@@ -76,8 +80,31 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                 b = rp[r + 1];
             }
             Acc<VT> acc[KPL];
-#pragma unroll 4
-            for (int j = a + e; j < b; j += es) {
+            int j = a + e;
+            // U elements at a time: all value and column loads first, then all gathers, so
+            // U memory round trips overlap instead of running one after another
+            for (; j + (U - 1) * es < b; j += U * es) {
+                VT val[U];
+                int col[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    val[u] = ld_val(v + j + u * es, pf);
+                    col[u] = ld_col(ci + j + u * es, pf);
+                }
+                VT xv[U][KPL];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const VT *xr = X + (long long)col[u] * ldx + cl;
+#pragma unroll
+                    for (int p = 0; p < KPL; ++p) xv[u][p] = colok[p] ? ld_x(xr + p * kc, pl) : VT(0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int p = 0; p < KPL; ++p)
+                        if (colok[p]) acc[p].add(val[u], xv[u][p]);
+            }
+            for (; j < b; j += es) {
                 const VT val = ld_val(v + j, pf);
                 const VT *xr = X + (long long)ld_col(ci + j, pf) * ldx + cl;
 #pragma unroll
@@ -108,7 +135,8 @@ cudaError_t launch_group(const Handle &h, const void *X, long long ldx, void *Y,
     const int tr = h.rows_per_tile;
     const long long ntiles = ((long long)h.m + tr - 1) / tr;
     const long long want = (ntiles + (GROUP_THREADS / 32) - 1) / (GROUP_THREADS / 32);
-    const long long cap = (long long)h.sm_count * GROUP_MINB;
+    const int minb = kpl == 1 ? group_minb<1>() : (kpl == 2 ? group_minb<2>() : group_minb<4>());
+    const long long cap = (long long)h.sm_count * minb;
     const unsigned grid = (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
     (void)gpw;
     const int gs = ilog2(gl), ks = ilog2(kc);
