@@ -5,6 +5,7 @@
 * ``pava_b200/lib/libpava_gpu.so``  -- the CUDA engine and its C ABI (include/pava_gpu.h)
 * ``pava_b200/lib/libpava_host.so`` -- host-side C++: seeded matrix generators, the Matrix
   Market reader/writer and the COO->CSR conversion (include/pava_host.h)
+* ``pava_b200/lib/pava_bench``      -- main.cpp's CVR / CSR5 benchmark loop over the C ABI
 
 nvcc cross-compiles for sm_100a without a GPU, so this runs on any machine with the CUDA
 toolkit.  CUDA runtime is linked statically, so the library does not depend on the
@@ -75,9 +76,23 @@ def build_host(force: bool = False) -> str:
     return out
 
 
+def build_driver(force: bool = False) -> str:
+    """pava_bench: main.cpp's CVR / CSR5 benchmark loop over the C ABI (csrc/host/pava_bench.cpp)."""
+    out = os.path.join(LIBDIR, "pava_bench")
+    src = os.path.join(CSRC, "host", "pava_bench.cpp")
+    deps = [src, os.path.join(LIBDIR, "libpava_gpu.so"), os.path.join(LIBDIR, "libpava_host.so"),
+            os.path.join(ROOT, "include", "pava_gpu.h"), os.path.join(ROOT, "include", "pava_host.h")]
+    if not force and not _stale(out, deps):
+        return out
+    _run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), src, "-o", out,
+          "-L", LIBDIR, "-lpava_gpu", "-lpava_host", "-Wl,-rpath,$ORIGIN"])
+    return out
+
+
 def build(force: bool = False) -> None:
     build_host(force)
     build_gpu(force)
+    build_driver(force)
 
 
 if __name__ == "__main__":

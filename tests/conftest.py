@@ -15,8 +15,7 @@ def pytest_configure(config):
 
 def _ensure_built():
     from pava_b200 import build as B
-    B.build_host()
-    B.build_gpu()
+    B.build()
     if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True)
 
