@@ -80,7 +80,13 @@ typedef struct pava_opts {
     int cols_per_lane;    /* CSR, pava_spmm: right-hand sides per lane, 1, 2 or 4; needs
                              col_lanes * cols_per_lane >= k (default: from k) */
     int rows_per_tile;    /* CSR: rows per warp tile of the persistent launch, a multiple of
-                             32 / lanes_per_row (default: 4 row groups) */
+                             32 / lanes_per_row (default: 4 row groups); with x_window, rows
+                             per 256-thread CTA tile, a multiple of 8 * 32 / lanes_per_row
+                             (default: 4 passes of the CTA's row groups) */
+    int x_window;         /* CSR, pava_spmm: 1 = each CTA copies its row tile's column window
+                             of X into shared memory (up to 100 KB) and reads X from there;
+                             for banded / local matrices.  Tiles whose window is wider read X
+                             from global memory. */
 } pava_opts;
 
 typedef struct pava_info {
@@ -188,7 +194,7 @@ pava_status pava_batch_destroy(pava_batch *b);
  * warm-up calls, then the median of `reps` CUDA-event timings of the SpMV/SpMM with x and y
  * already on the device).  Candidates: for k = 1, CVR steps 64/128 and CSR5 sigma 16/32; for
  * every k, the CSR row-group form over lanes_per_row x col_lanes x cols_per_lane x
- * rows_per_tile.  entries[0 .. *n_entries) receive every candidate (ms < 0 when it failed,
+ * rows_per_tile, and for k > 1 also with x_window.  entries[0 .. *n_entries) receive every candidate (ms < 0 when it failed,
  * with its status), *best the index of the fastest.  No counterpart in the reference. */
 typedef struct pava_tune_entry {
     int format;

@@ -46,7 +46,8 @@ class PavaCsr(ctypes.Structure):
 class PavaOpts(ctypes.Structure):
     _fields_ = [("steps", c_int), ("sigma", c_int), ("tiles_per_chunk", c_int),
                 ("precision", c_int), ("index_mode", c_int), ("lanes_per_row", c_int),
-                ("col_lanes", c_int), ("cols_per_lane", c_int), ("rows_per_tile", c_int)]
+                ("col_lanes", c_int), ("cols_per_lane", c_int), ("rows_per_tile", c_int),
+                ("x_window", c_int)]
 
 
 class PavaInfo(ctypes.Structure):

@@ -45,7 +45,7 @@ class SpMatrix:
                  tiles_per_chunk: int = 0, precision: int = _abi.PREC_FP64,
                  index_mode: int = _abi.INDEX_I32, lanes_per_row: int = 0,
                  col_lanes: int = 0, cols_per_lane: int = 0, rows_per_tile: int = 0,
-                 stream=None, device_arrays=None):
+                 x_window: int = 0, stream=None, device_arrays=None):
         L = _abi.gpu()
         self.m, self.n, self.nnz = A.m, A.n, A.nnz
         self.format = format
@@ -64,7 +64,7 @@ class SpMatrix:
             csr.vals = self._keep[2].ctypes.data
             csr.on_device = 0
         opts = _abi.PavaOpts(steps, sigma, tiles_per_chunk, precision, index_mode, lanes_per_row,
-                             col_lanes, cols_per_lane, rows_per_tile)
+                             col_lanes, cols_per_lane, rows_per_tile, x_window)
         h = _abi.c_void_p()
         _abi.check(L.pava_create(ctypes.byref(csr), FORMATS[format], ctypes.byref(opts),
                                  _abi.c_void_p(_stream_ptr(stream) if stream is not None else None),

@@ -108,9 +108,11 @@ bool resolve_group_shape(const pava::Handle &h, int k, pava::Handle &out, std::s
         return false;
     }
     const int gpw = 32 / gl;
-    int tr = h.rows_per_tile ? h.rows_per_tile : 4 * gpw;
-    if (tr % gpw != 0) {
-        why = "rows_per_tile must be a multiple of 32 / lanes_per_row";
+    const int unit = h.x_window ? 8 * gpw : gpw;  // rows one pass of a warp / of a CTA covers
+    int tr = h.rows_per_tile ? h.rows_per_tile : 4 * unit;
+    if (tr % unit != 0) {
+        why = h.x_window ? "rows_per_tile must be a multiple of 8 * 32 / lanes_per_row with x_window"
+                         : "rows_per_tile must be a multiple of 32 / lanes_per_row";
         return false;
     }
     out.lanes_per_row = gl;
@@ -296,6 +298,7 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
         h.col_lanes = o.col_lanes;
         h.cols_per_lane = o.cols_per_lane;
         h.rows_per_tile = o.rows_per_tile;
+        h.x_window = o.x_window ? 1 : 0;
         std::string why;
         pava::Handle probe;
         if ((o.lanes_per_row && !pow2_le32(o.lanes_per_row)) ||

@@ -170,7 +170,7 @@ pava_status build_union(int count, const pava_csr *mats, cudaStream_t s, pava_ba
     return PAVA_SUCCESS;
 }
 
-// Built-in candidate forms for k right-hand sides.
+// Built-in candidate forms for k right-hand sides (at most 72 for any k <= 128).
 std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
     std::vector<std::pair<int, pava_opts>> c;
     auto base = [&]() {
@@ -206,6 +206,17 @@ std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
                 o.rows_per_tile = groups * (32 / gl);
                 c.push_back({PAVA_FORMAT_CSR, o});
             }
+        if (k > 1)  // X windows in shared memory: CTA tiles of 128 or 256 rows
+            for (int gl = kc; gl <= 32; gl <<= 1)
+                for (int tr : {128, 256}) {
+                    pava_opts o = base();
+                    o.lanes_per_row = gl;
+                    o.col_lanes = kc;
+                    o.cols_per_lane = kpl;
+                    o.x_window = 1;
+                    o.rows_per_tile = tr;  // a multiple of 8 * 32 / gl for every gl >= 2
+                    c.push_back({PAVA_FORMAT_CSR, o});
+                }
     }
     return c;
 }

@@ -13,6 +13,8 @@
 // keeps one launch per SpMV/SpMM whatever the number of rows -- the batched path (a
 // block-diagonal union of many small matrices) relies on this.
 
+#include <climits>
+
 #include "k_stream.cuh"
 #include "pava_internal.h"
 
@@ -39,14 +41,61 @@ __device__ __forceinline__ int ld_col(const int *p, uint64_t pol) {
     return r;
 }
 
+// Rows shared by several column lanes (KC > 1): the group loads its row's nonzeros
+// cooperatively, GL at a time (lane gi loads element base + gi, one coalesced load per lane and
+// stream), with the next round's loads in flight while the current round is consumed; each
+// element reaches the lanes that need it by shuffle.  Slice e takes elements e, e + ES, ... in
+// ascending order, as the per-lane loop does, so the sums have the same bits.  The round count
+// is the maximum over the warp's groups so that every shuffle has all 32 lanes.
+template <int KPL, typename VT, typename XREAD>
+__device__ __forceinline__ void coop_row(int a, int b, int gi, int gl, int es, int e, int kc,
+                                         int lane, const int *__restrict__ ci,
+                                         const VT *__restrict__ v, const bool (&colok)[KPL],
+                                         XREAD xread, Acc<VT> (&acc)[KPL], uint64_t pf) {
+    int rounds = (b - a + gl - 1) / gl;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const int t = __shfl_xor_sync(FULL, rounds, o);
+        rounds = t > rounds ? t : rounds;
+    }
+    const int gbase = lane & ~(gl - 1);
+    VT pv = VT(0);
+    int pc = 0;
+    if (a + gi < b) {
+        pv = ld_val(v + a + gi, pf);
+        pc = ld_col(ci + a + gi, pf);
+    }
+    for (int rd = 0; rd < rounds; ++rd) {
+        const VT cv = pv;
+        const int cc = pc;
+        const int base = a + rd * gl;
+        if (base + gl + gi < b) {  // next round in flight
+            pv = ld_val(v + base + gl + gi, pf);
+            pc = ld_col(ci + base + gl + gi, pf);
+        }
+        for (int u = 0; u < kc; ++u) {
+            const int o = e + u * es;
+            const VT val = __shfl_sync(FULL, cv, gbase + o);
+            const int col = __shfl_sync(FULL, cc, gbase + o);
+            if (base + o < b) {
+#pragma unroll
+                for (int p = 0; p < KPL; ++p)
+                    if (colok[p]) acc[p].add(val, xread(col, p));
+            }
+        }
+    }
+}
+
 constexpr int GROUP_THREADS = 256;
 // resident blocks per SM: more warps in flight for the narrow shapes
 template <int KPL> constexpr int group_minb() { return KPL == 1 ? 6 : (KPL == 2 ? 5 : 4); }
+// resident blocks per SM of the cooperative (k > 1) shapes
+constexpr int COOP_MINB = 4;
 // elements in flight per lane
 template <int KPL> constexpr int group_unroll() { return KPL == 1 ? 4 : (KPL == 2 ? 2 : 1); }
 
-template <int KPL, typename VT>
-__global__ void __launch_bounds__(GROUP_THREADS, group_minb<KPL>())
+template <int KPL, typename VT, bool COOP>
+__global__ void __launch_bounds__(GROUP_THREADS, COOP ? COOP_MINB : group_minb<KPL>())
 csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                  const VT *__restrict__ v, const VT *__restrict__ X, long long ldx,
                  double *__restrict__ Y, long long ldy, int m, int k, int gl_shift,
@@ -81,6 +130,14 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             }
             Acc<VT> acc[KPL];
             int j = a + e;
+            if (COOP) {
+                coop_row<KPL>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
+                              [&](int col, int p) {
+                                  return ld_x(X + (long long)col * ldx + cl + p * kc, pl);
+                              },
+                              acc, pf);
+                j = b;
+            }
             // U elements at a time: all value and column loads first, then all gathers, so
             // U memory round trips overlap instead of running one after another
             for (; j + (U - 1) * es < b; j += U * es) {
@@ -121,21 +178,208 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
     }
 }
 
+// Windowed variant for k > 1 on matrices whose rows reach a narrow column range (banded,
+// stencil-like): a CTA owns a tile of TR consecutive rows, finds the tile's column window
+// [cmin, cmax], copies X[cmin .. cmax][0 .. k) into shared memory once, and its row groups
+// read X from there.  Each X row is then fetched from L2 once per tile instead of once per
+// nonzero that references it.  Tiles whose window does not fit take the global gathers.
+constexpr int WINDOW_MINB = 2;
+constexpr int WINDOW_SMEM = 100 * 1024;  // bytes of X per CTA (two CTAs per SM)
+
+template <int KPL, typename VT>
+__global__ void __launch_bounds__(GROUP_THREADS, WINDOW_MINB)
+csr_window_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
+                  const VT *__restrict__ v, const VT *__restrict__ X, long long ldx,
+                  double *__restrict__ Y, long long ldy, int m, int k, int gl_shift,
+                  int kc_shift, int tile_rows, int max_w) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    VT *xs = reinterpret_cast<VT *>(smem_raw);
+    constexpr int WARPS = GROUP_THREADS / 32;
+    __shared__ int s_min[WARPS], s_max[WARPS];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int gl = 1 << gl_shift, kc = 1 << kc_shift;
+    const int grp = lane >> gl_shift;
+    const int gpw = 32 >> gl_shift;
+    const int gi = lane & (gl - 1);
+    const int e = gi >> kc_shift;
+    const int es = gl >> kc_shift;
+    const int cl = gi & (kc - 1);
+    const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+    const long long ntiles = ((long long)m + tile_rows - 1) / tile_rows;
+    const int rows_per_pass = WARPS * gpw;
+
+    bool colok[KPL];
+#pragma unroll
+    for (int p = 0; p < KPL; ++p) colok[p] = cl + p * kc < k;
+
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const long long r0 = t * tile_rows;
+        const long long r1 = r0 + tile_rows < m ? r0 + tile_rows : m;
+        // the tile's column window
+        const int j0 = rp[r0], j1 = rp[r1];
+        int cmin = INT_MAX, cmax = -1;
+        for (int j = j0 + tid; j < j1; j += GROUP_THREADS) {
+            const int c = ci[j];
+            cmin = c < cmin ? c : cmin;
+            cmax = c > cmax ? c : cmax;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const int a = __shfl_xor_sync(FULL, cmin, o), b = __shfl_xor_sync(FULL, cmax, o);
+            cmin = a < cmin ? a : cmin;
+            cmax = b > cmax ? b : cmax;
+        }
+        if (lane == 0) {
+            s_min[w] = cmin;
+            s_max[w] = cmax;
+        }
+        __syncthreads();
+        cmin = s_min[0];
+        cmax = s_max[0];
+#pragma unroll
+        for (int q = 1; q < WARPS; ++q) {
+            cmin = s_min[q] < cmin ? s_min[q] : cmin;
+            cmax = s_max[q] > cmax ? s_max[q] : cmax;
+        }
+        const int W = cmax >= cmin ? cmax - cmin + 1 : 0;
+        const bool staged = W > 0 && W <= max_w;
+        if (staged) {  // X[cmin .. cmax][0 .. k) -> xs, row stride k; SU loads in flight
+            constexpr int SU = 8;
+            const int total = W * k;  // <= WINDOW_SMEM / sizeof(VT)
+            const VT *src = X + (long long)cmin * ldx;
+            for (int q0 = tid; q0 < total; q0 += SU * GROUP_THREADS) {
+                VT t[SU];
+#pragma unroll
+                for (int u = 0; u < SU; ++u) {
+                    const int q = q0 + u * GROUP_THREADS;
+                    if (q < total) {
+                        if (ldx == k) {
+                            t[u] = ld_x(src + q, pl);
+                        } else {
+                            const int wr = q / k;
+                            t[u] = ld_x(src + (long long)wr * ldx + (q - wr * k), pl);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < SU; ++u) {
+                    const int q = q0 + u * GROUP_THREADS;
+                    if (q < total) xs[q] = t[u];
+                }
+            }
+        }
+        __syncthreads();
+        for (long long rb = r0; rb < r1; rb += rows_per_pass) {
+            const long long r = rb + (long long)w * gpw + grp;
+            const bool valid = r < r1;
+            int a = 0, b = 0;
+            if (valid) {
+                a = rp[r];
+                b = rp[r + 1];
+            }
+            Acc<VT> acc[KPL];
+            int j = a + e;
+            if (kc > 1) {
+                if (staged)
+                    coop_row<KPL>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
+                                  [&](int col, int p) { return xs[(col - cmin) * k + cl + p * kc]; },
+                                  acc, pf);
+                else
+                    coop_row<KPL>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
+                                  [&](int col, int p) {
+                                      return ld_x(X + (long long)col * ldx + cl + p * kc, pl);
+                                  },
+                                  acc, pf);
+                j = b;
+            } else if (staged) {  // WU elements' values and columns in flight, then the shared reads
+                constexpr int WU = 4;
+                for (; j + (WU - 1) * es < b; j += WU * es) {
+                    VT val[WU];
+                    int col[WU];
+#pragma unroll
+                    for (int u = 0; u < WU; ++u) {
+                        val[u] = ld_val(v + j + u * es, pf);
+                        col[u] = ld_col(ci + j + u * es, pf);
+                    }
+#pragma unroll
+                    for (int u = 0; u < WU; ++u) {
+                        const VT *xr = xs + (col[u] - cmin) * k + cl;
+#pragma unroll
+                        for (int p = 0; p < KPL; ++p)
+                            if (colok[p]) acc[p].add(val[u], xr[p * kc]);
+                    }
+                }
+            }
+            for (; j < b; j += es) {
+                const VT val = ld_val(v + j, pf);
+                const int col = ld_col(ci + j, pf);
+                if (staged) {
+                    const VT *xr = xs + (col - cmin) * k + cl;
+#pragma unroll
+                    for (int p = 0; p < KPL; ++p)
+                        if (colok[p]) acc[p].add(val, xr[p * kc]);
+                } else {
+                    const VT *xr = X + (long long)col * ldx + cl;
+#pragma unroll
+                    for (int p = 0; p < KPL; ++p)
+                        if (colok[p]) acc[p].add(val, ld_x(xr + p * kc, pl));
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < KPL; ++p) {
+                double s = acc[p].value();
+                for (int o = kc; o < gl; o <<= 1) s += __shfl_xor_sync(FULL, s, o);
+                if (valid && e == 0 && colok[p]) Y[r * ldy + cl + p * kc] = s;
+            }
+        }
+        __syncthreads();  // xs is restaged by the next tile
+    }
+}
+
 int ilog2(int v) {
     int s = 0;
     while ((1 << s) < v) ++s;
     return s;
 }
 
+template <int KPL, typename VT>
+cudaError_t launch_window(const Handle &h, const VT *x, long long ldx, double *y, long long ldy,
+                          int k, cudaStream_t s) {
+    const int tr = h.rows_per_tile;
+    const long long ntiles = ((long long)h.m + tr - 1) / tr;
+    const long long cap = (long long)h.sm_count * WINDOW_MINB;
+    const unsigned grid = (unsigned)(ntiles < cap ? (ntiles > 0 ? ntiles : 1) : cap);
+    const int max_w = (int)(WINDOW_SMEM / ((size_t)k * sizeof(VT)));
+    const size_t smem = (size_t)max_w * k * sizeof(VT);
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        csr_window_kernel<KPL, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WINDOW_SMEM);
+    if (attr != cudaSuccess) return attr;
+    csr_window_kernel<KPL, VT><<<grid, GROUP_THREADS, smem, s>>>(
+        h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, ilog2(h.lanes_per_row),
+        ilog2(h.col_lanes), tr, max_w);
+    return cudaGetLastError();
+}
+
 template <typename VT>
 cudaError_t launch_group(const Handle &h, const void *X, long long ldx, void *Y, long long ldy,
                          int k, cudaStream_t s) {
     const int gl = h.lanes_per_row, kc = h.col_lanes, kpl = h.cols_per_lane;
+    if (h.x_window) {
+        const VT *x = (const VT *)X;
+        double *y = (double *)Y;
+        switch (kpl) {
+            case 1: return launch_window<1, VT>(h, x, ldx, y, ldy, k, s);
+            case 2: return launch_window<2, VT>(h, x, ldx, y, ldy, k, s);
+            case 4: return launch_window<4, VT>(h, x, ldx, y, ldy, k, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     const int gpw = 32 / gl;
     const int tr = h.rows_per_tile;
     const long long ntiles = ((long long)h.m + tr - 1) / tr;
     const long long want = (ntiles + (GROUP_THREADS / 32) - 1) / (GROUP_THREADS / 32);
-    const int minb = kpl == 1 ? group_minb<1>() : (kpl == 2 ? group_minb<2>() : group_minb<4>());
+    const int minb = kc > 1 ? COOP_MINB
+                            : (kpl == 1 ? group_minb<1>() : (kpl == 2 ? group_minb<2>() : group_minb<4>()));
     const long long cap = (long long)h.sm_count * minb;
     const unsigned grid = (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
     (void)gpw;
@@ -143,21 +387,21 @@ cudaError_t launch_group(const Handle &h, const void *X, long long ldx, void *Y,
     const VT *x = (const VT *)X;
     const VT *v = (const VT *)h.v;
     double *y = (double *)Y;
+    const bool coop = kc > 1;
+#define PAVA_GROUP_LAUNCH(KPLV)                                                               \
+    if (coop)                                                                                 \
+        csr_group_kernel<KPLV, VT, true><<<grid, GROUP_THREADS, 0, s>>>(                      \
+            h.rp, h.ci, v, x, ldx, y, ldy, h.m, k, gs, ks, tr);                               \
+    else                                                                                      \
+        csr_group_kernel<KPLV, VT, false><<<grid, GROUP_THREADS, 0, s>>>(                     \
+            h.rp, h.ci, v, x, ldx, y, ldy, h.m, k, gs, ks, tr);
     switch (kpl) {
-        case 1:
-            csr_group_kernel<1, VT><<<grid, GROUP_THREADS, 0, s>>>(h.rp, h.ci, v, x, ldx, y, ldy,
-                                                                 h.m, k, gs, ks, tr);
-            break;
-        case 2:
-            csr_group_kernel<2, VT><<<grid, GROUP_THREADS, 0, s>>>(h.rp, h.ci, v, x, ldx, y, ldy,
-                                                                 h.m, k, gs, ks, tr);
-            break;
-        case 4:
-            csr_group_kernel<4, VT><<<grid, GROUP_THREADS, 0, s>>>(h.rp, h.ci, v, x, ldx, y, ldy,
-                                                                 h.m, k, gs, ks, tr);
-            break;
+        case 1: PAVA_GROUP_LAUNCH(1) break;
+        case 2: PAVA_GROUP_LAUNCH(2) break;
+        case 4: PAVA_GROUP_LAUNCH(4) break;
         default: return cudaErrorInvalidValue;
     }
+#undef PAVA_GROUP_LAUNCH
     return cudaGetLastError();
 }
 

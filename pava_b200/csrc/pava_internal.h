@@ -41,7 +41,9 @@ struct Handle {
     int lanes_per_row = 0;   // plain CSR: lanes per row group (GL)
     int col_lanes = 1;       //   lanes across the right-hand sides (KC)
     int cols_per_lane = 1;   //   right-hand sides per lane (KPL)
-    int rows_per_tile = 0;   //   rows per warp tile of the persistent launch (TR)
+    int rows_per_tile = 0;   //   rows per warp tile of the persistent launch (TR), or per
+                             //   CTA tile with x_window
+    int x_window = 0;        //   stage each CTA tile's window of X in shared memory
     int device = 0, sm_count = 0;
 
     int *arp = nullptr;            // augmented row pointer, m + 2 entries (row m = padding)

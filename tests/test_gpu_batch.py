@@ -46,6 +46,37 @@ def test_spmm_banded_shapes(cuda, k, gl, kc, kpl, tr):
     _check_cols(A, X, Y, TOL)
 
 
+WINDOW = [  # (k, lanes_per_row, col_lanes, cols_per_lane, rows_per_tile)
+    (8, 8, 8, 1, 0), (8, 8, 4, 2, 32), (32, 32, 32, 1, 8), (32, 8, 8, 4, 128),
+    (13, 16, 16, 1, 0), (2, 4, 2, 1, 256), (64, 32, 32, 2, 0),
+]
+
+
+@pytest.mark.parametrize("k,gl,kc,kpl,tr", WINDOW, ids=[f"k{s[0]}_g{s[1]}_c{s[2]}_p{s[3]}_t{s[4]}" for s in WINDOW])
+def test_spmm_x_window(cuda, k, gl, kc, kpl, tr):
+    """X windows staged in shared memory: banded rows (every tile staged), power-law rows
+    (wide windows: the global-gather fallback) and a ragged last tile."""
+    torch = cuda
+    for A in (M.banded(20_003, 64, 24, seed=31), M.powerlaw(9_001, mean=10.0, p_empty=0.05, seed=32)):
+        X, Xd = _x(torch, A.n, k, seed=33)
+        mat = SpMatrix(A, "csr", lanes_per_row=gl, col_lanes=kc, cols_per_lane=kpl,
+                       rows_per_tile=tr, x_window=1)
+        Y = mat.spmm(Xd).cpu().numpy()
+        _check_cols(A, X, Y, TOL)
+        # the same arithmetic order as the global-gather kernel: identical bits
+        ref = SpMatrix(A, "csr", lanes_per_row=gl, col_lanes=kc, cols_per_lane=kpl).spmm(Xd)
+        assert np.array_equal(Y, ref.cpu().numpy())
+
+
+def test_spmm_x_window_fp32c(cuda):
+    torch = cuda
+    A = M.stencil27(24, seed=34)
+    X, Xd = _x(torch, A.n, 16, seed=35, fp32=True)
+    mat = SpMatrix(A, "csr", precision=_abi.PREC_FP32C, lanes_per_row=16, col_lanes=16,
+                   x_window=1)
+    _check_cols(A, X, mat.spmm(Xd).cpu().numpy(), TOL32)
+
+
 def test_spmm_irregular_rows_and_strides(cuda):
     torch = cuda
     A = M.powerlaw(30_000, mean=16.0, cap=5_000, p_empty=0.05, seed=13)
@@ -82,8 +113,10 @@ def test_spmm_fp32c(cuda):
 
 @pytest.mark.parametrize("kw", [dict(lanes_per_row=3), dict(col_lanes=64),
                                 dict(cols_per_lane=3), dict(lanes_per_row=4, col_lanes=8),
-                                dict(lanes_per_row=4, rows_per_tile=3)],
-                         ids=["gl3", "kc64", "kpl3", "kc_gt_gl", "tr_not_multiple"])
+                                dict(lanes_per_row=4, rows_per_tile=3),
+                                dict(lanes_per_row=8, rows_per_tile=8, x_window=1)],
+                         ids=["gl3", "kc64", "kpl3", "kc_gt_gl", "tr_not_multiple",
+                              "window_tr_not_multiple"])
 def test_csr_shape_rejected(cuda, kw):
     A = M.random_csr(1000, seed=19)
     with pytest.raises(_abi.PavaError) as e:
