@@ -288,6 +288,17 @@ pava_status pava_select(pava_mlp *m, const pava_csr *A, int *variant, float *pre
 pava_status pava_create_selected(const pava_csr *A, pava_mlp *m, void *stream,
                                  pava_handle **out, int *variant);
 
+/* COO -> CSR on the device: the loader's conversion (readCOOMatrix's symmetric expansion and
+ * 1-based shift, utils/basicMatrix.cpp:63-253; convertCOO2CSR via mkl_dcsrcoo, :350-415).
+ * rows / cols / vals are device arrays of nnz entries with index base 0 or 1; symmetric = 1
+ * adds (c, r) for every off-diagonal (r, c).  The result has ascending rows and ascending
+ * columns inside each row, duplicates kept as separate entries in input order (the same as
+ * pava_coo_to_csr of pava_host.h); it is allocated on the device -- free it with
+ * pava_free_device_csr.  Indices outside the matrix give PAVA_E_INVALID_CSR. */
+pava_status pava_coo_to_csr_device(int m, int n, long long nnz, const int *rows,
+                                   const int *cols, const double *vals, int index_base,
+                                   int symmetric, void *stream, pava_csr *out);
+
 /* Drop-ins for the reference's engine entry points, same signatures and meaning:
  * conduct_cvr (cvr/cvr.h:1953) and conduct_csr5 (csr5/csr5.h:72-74).  Each copies the CSR to
  * the device, converts (timed as the convert column), runs one SpMV into refOut / y (the

@@ -122,6 +122,8 @@ GPU_SYMBOLS = [
                             c_void_p]),
     ("pava_create_selected", c_int, [ctypes.POINTER(PavaCsr), c_void_p, c_void_p,
                                      ctypes.POINTER(c_void_p), ctypes.POINTER(c_int)]),
+    ("pava_coo_to_csr_device", c_int, [c_int, c_int, c_ll, c_void_p, c_void_p, c_void_p, c_int,
+                                       c_int, c_void_p, ctypes.POINTER(PavaCsr)]),
     ("conduct_cvr_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_int, c_char_p, c_int]),
     ("conduct_csr5_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,

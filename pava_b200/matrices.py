@@ -156,3 +156,34 @@ def read_mtx(path: str) -> CSR:
 
 def write_mtx(path: str, A: CSR) -> None:
     _rc(_abi.host().pava_mtx_write(path.encode(), A.m, A.n, _p(A.rp), _p(A.ci), _p(A.v)))
+
+
+def coo_to_csr_device(m: int, n: int, rows, cols, vals, index_base: int = 0,
+                      symmetric: bool = False):
+    """COO on the GPU -> sorted CSR on the GPU (pava_coo_to_csr_device).  rows / cols are
+    int32 CUDA tensors, vals a float64 CUDA tensor.  Returns (rp, ci, v) CUDA tensors."""
+    import torch
+    A = _abi.PavaCsr()
+    _abi.check(_abi.gpu().pava_coo_to_csr_device(m, n, rows.numel(), rows.data_ptr(),
+                                                 cols.data_ptr(), vals.data_ptr(), index_base,
+                                                 int(symmetric), None, A))
+    try:
+        out = []
+        for ptr, cnt, ts, dt in ((A.row_ptr, m + 1, "<i4", torch.int32),
+                                 (A.col_idx, A.nnz, "<i4", torch.int32),
+                                 (A.vals, A.nnz, "<f8", torch.float64)):
+            t = torch.empty(cnt, dtype=dt, device="cuda")
+            if cnt:
+                t.copy_(torch.as_tensor(_DevView(ptr, cnt, ts), device="cuda"))
+            out.append(t)
+        return tuple(out)
+    finally:
+        _abi.gpu().pava_free_device_csr(A)
+
+
+class _DevView:
+    """A device buffer seen through the CUDA array interface (no copy)."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3}
