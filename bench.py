@@ -140,6 +140,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(values, world, device):
+    """Max over the ranks of each timing; every rank calls it with the same number of values,
+    in the same order (a collective)."""
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def aggregate_gbps(world, alg_bytes, ms):
+    """Whole-job throughput of `world` replicas that each move alg_bytes per step in (at
+    most) ms milliseconds."""
+    return world * alg_bytes / (ms * 1e-3) / 1e9
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -278,10 +294,7 @@ def main():
         barrier()
     ms = start.elapsed_time(stop) / K
     main_ms = sum(a.elapsed_time(b) for a, b in ev) / K
-    t = torch.tensor([ms, main_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms, main_ms = float(t[0]), float(t[1])
+    ms, main_ms = max_over_ranks([ms, main_ms], world, dev)
 
     # correctness of the timed variant (relative error against a long-double CSR product is
     # checked by the test suite; here the plain CSR kernel is the in-run check)
@@ -314,10 +327,7 @@ def main():
     eb.record(stream)
     eb.synchronize()
     e2e_ms = ea.elapsed_time(eb) / KE
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_ms = float(te[0])
+    e2e_ms, = max_over_ranks([e2e_ms], world, dev)
 
     peak, peak_kind = peak_hbm()
     achieved = alg / (main_ms * 1e-3) / 1e9
@@ -330,7 +340,7 @@ def main():
             cpu = cpu_baseline(A, x_host, alg)
         line = {
             "metric": METRIC,
-            "value": round(world * alg / (ms * 1e-3) / 1e9, 3),
+            "value": round(aggregate_gbps(world, alg, ms), 3),
             "unit": "GB/s",
             "n_gpus": world,
             "steps": K,
@@ -357,7 +367,7 @@ def main():
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "kernel": kernel_key, "kernel_ms": round(main_ms, 6)},
-            "e2e": {"value": round(world * alg / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GB/s",
+            "e2e": {"value": round(aggregate_gbps(world, alg, e2e_ms), 3), "unit": "GB/s",
                     "ms_per_step": round(e2e_ms, 6), "h2d_bytes_per_step": 8 * A.n,
                     "d2h_bytes_per_step": 8 * A.m},
             "gpu_launches": 2 * K,
