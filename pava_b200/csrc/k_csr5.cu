@@ -114,6 +114,13 @@ constexpr int SPMV_WARPS = 8;
 
 // CSR5 SpMV: one warp per chunk of G tiles, walked as one pipelined run of 4-step blocks
 // (values two blocks ahead, columns three, x one); tile descriptors one tile ahead.
+//
+// Row ends inside a tile: when no lane of the warp starts more than KSTK rows in the tile
+// (the usual case), an element that starts a row parks the lane's finished piece in the
+// lane's next shared-memory slot (a predicated store) and restarts the accumulator (a select),
+// so the step has no branch; at the tile end piece 0 (the end of the row the lane started
+// with) joins the cross-lane combine and pieces 1 .. k-1, rows that start and end in the
+// lane, go to y.  Other tiles write each finished row as it ends.
 template <int SIGMA, typename VT, typename IT>
 __global__ void __launch_bounds__(SPMV_WARPS * 32, sizeof(VT) == 8 ? PAVA_CSR5_MINB : PAVA_CSR5_MINB32)
 csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_ptr,
@@ -126,6 +133,10 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
     const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
     const long long nwarps = (long long)gridDim.x * SPMV_WARPS;
     (void)w;
+    constexpr int KSTK = 4;
+    constexpr unsigned SLOT = SPMV_WARPS * 32 * 8;  // bytes between a thread's slots
+    __shared__ __align__(16) double s_piece[KSTK * SPMV_WARPS * 32];
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(&s_piece[threadIdx.x]);
 
     for (long long c = (long long)blockIdx.x * SPMV_WARPS + w; c < nchunks; c += nwarps) {
         const ChunkHdr H = hdr[c];
@@ -156,6 +167,9 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
         double hpiece = 0.0;
         bool seen = false;
         int tt = 0;
+        bool fast = false;
+        int nst = 0, row0 = 0;
+        unsigned sp = sbase;
 #pragma unroll 1
         for (int blk = 0; blk < NB; ++blk) {
             CBlk<IT> cn = c2;
@@ -176,30 +190,50 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
                     rsn = tile_ptr[t0 + tt + 1];
                 }
                 b00 = (int)(__shfl_sync(FULL, F, 0) & 1u);
-                const int nst = __popc(F);
+                nst = __popc(F);
                 const int excl = warp_excl_scan(nst, lane);
                 total = __shfl_sync(FULL, excl + nst, 31);
                 rowcur = rs + excl - b00;  // row open when the lane starts
+                row0 = rowcur;
                 acc.reset();
                 hpiece = 0.0;
                 seen = false;
+                fast = !__any_sync(FULL, nst > KSTK);
+                sp = sbase;
             }
+            const unsigned Fb = F >> (qb * 4);
+            if (fast) {  // row ends park the piece in the lane's shared slots: no branch
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int i = qb * 4 + q;
-                if ((F >> i) & 1u) {
-                    if (seen) {
-                        if (rowcur < m) y[rowcur] = acc.value();
-                    } else {
-                        hpiece = acc.value();
-                        seen = true;
-                    }
-                    ++rowcur;
-                    acc.reset();
+                for (int q = 0; q < 4; ++q) {
+                    const bool st = (Fb >> q) & 1u;
+                    acc.push(sp, st);
+                    sp += st ? SLOT : 0u;
+                    acc.add_restart(v0.get(q), x0[q], st);
                 }
-                acc.add(v0.get(q), x0[q]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if ((Fb >> q) & 1u) {
+                        if (seen) {
+                            if (rowcur < m) y[rowcur] = acc.value();
+                        } else {
+                            hpiece = acc.value();
+                            seen = true;
+                        }
+                        ++rowcur;
+                        acc.reset();
+                    }
+                    acc.add(v0.get(q), x0[q]);
+                }
             }
             if (qb == NBT - 1) {  // tile end: combine the lanes' open pieces
+                if (fast) {
+                    seen = nst > 0;
+                    if (seen) hpiece = Acc<VT>::piece_at(sbase);
+                    for (int k2 = 1; k2 < nst; ++k2)
+                        if (row0 + k2 < m) y[row0 + k2] = Acc<VT>::piece_at(sbase + k2 * SLOT);
+                    rowcur = row0 + nst;
+                }
                 if (!seen) hpiece = acc.value();
                 const double tl = seen ? acc.value() : 0.0;
                 const unsigned sm = __ballot_sync(FULL, seen);

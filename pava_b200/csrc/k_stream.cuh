@@ -82,13 +82,45 @@ __host__ __device__ __forceinline__ long long cols_offset(int i, int k) {
 }
 
 template <typename VT> struct Acc;
+// Predicated shared-memory stores and loads of a parked row piece (shared-window addresses).
+__device__ __forceinline__ void sts_pred(unsigned addr, double v, bool p) {
+    asm volatile("{ .reg .pred q; setp.ne.u32 q, %2, 0; @q st.shared.f64 [%0], %1; }"
+                 :: "r"(addr), "d"(v), "r"((unsigned)p) : "memory");
+}
+__device__ __forceinline__ void sts_pred(unsigned addr, float a, float b, bool p) {
+    asm volatile("{ .reg .pred q; setp.ne.u32 q, %3, 0; @q st.shared.v2.f32 [%0], {%1, %2}; }"
+                 :: "r"(addr), "f"(a), "f"(b), "r"((unsigned)p) : "memory");
+}
+__device__ __forceinline__ double lds_f64(unsigned addr) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr) : "memory");
+    return v;
+}
+__device__ __forceinline__ float2 lds_v2f32(unsigned addr) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+    return v;
+}
+
+// Row accumulators.  push parks the current piece at a shared address when p is set,
+// piece_at reads one back as FP64, add_restart(v, x, st) starts a new sum at v*x when st is set.
 template <> struct Acc<double> {
+    __device__ __forceinline__ void push(unsigned addr, bool p) const { sts_pred(addr, s, p); }
+    __device__ __forceinline__ static double piece_at(unsigned addr) { return lds_f64(addr); }
+    __device__ __forceinline__ void add_restart(double v, double x, bool st) {
+        s = fma(v, x, st ? 0.0 : s);
+    }
     double s = 0.0;
     __device__ __forceinline__ void add(double v, double x) { s = fma(v, x, s); }
     __device__ __forceinline__ double value() const { return s; }
     __device__ __forceinline__ void reset() { s = 0.0; }
 };
 template <> struct Acc<float> {
+    __device__ __forceinline__ void push(unsigned addr, bool p) const { sts_pred(addr, s, c, p); }
+    __device__ __forceinline__ static double piece_at(unsigned addr) {
+        const float2 v = lds_v2f32(addr);
+        return (double)v.x + (double)v.y;
+    }
     float s = 0.f, c = 0.f;
     __device__ __forceinline__ void add(float v, float x) {
         const float p = v * x;
@@ -98,6 +130,11 @@ template <> struct Acc<float> {
         const float err = (s - (t - z)) + (p - z);
         s = t;
         c += err + e;
+    }
+    __device__ __forceinline__ void add_restart(float v, float x, bool st) {
+        s = st ? 0.f : s;
+        c = st ? 0.f : c;
+        add(v, x);
     }
     __device__ __forceinline__ double value() const { return (double)s + (double)c; }
     __device__ __forceinline__ void reset() { s = 0.f; c = 0.f; }
