@@ -14,6 +14,7 @@
 // block-diagonal union of many small matrices) relies on this.
 
 #include <climits>
+#include <type_traits>
 
 #include "k_stream.cuh"
 #include "pava_internal.h"
@@ -41,13 +42,14 @@ __device__ __forceinline__ int ld_col(const int *p, uint64_t pol) {
     return r;
 }
 
-// Rows shared by several column lanes (KC > 1): the group loads its row's nonzeros
+// Rows shared by several column lanes (KCT = KC > 1, a compile-time count so that the KC
+// elements of a round unroll): the group loads its row's nonzeros
 // cooperatively, GL at a time (lane gi loads element base + gi, one coalesced load per lane and
 // stream), with the next round's loads in flight while the current round is consumed; each
 // element reaches the lanes that need it by shuffle.  Slice e takes elements e, e + ES, ... in
 // ascending order, as the per-lane loop does, so the sums have the same bits.  The round count
 // is the maximum over the warp's groups so that every shuffle has all 32 lanes.
-template <int KPL, typename VT, typename XREAD>
+template <int KPL, int KCT, typename VT, typename XREAD>
 __device__ __forceinline__ void coop_row(int a, int b, int gi, int gl, int es, int e, int kc,
                                          int lane, const int *__restrict__ ci,
                                          const VT *__restrict__ v, const bool (&colok)[KPL],
@@ -73,7 +75,8 @@ __device__ __forceinline__ void coop_row(int a, int b, int gi, int gl, int es, i
             pv = ld_val(v + base + gl + gi, pf);
             pc = ld_col(ci + base + gl + gi, pf);
         }
-        for (int u = 0; u < kc; ++u) {
+#pragma unroll
+        for (int u = 0; u < KCT; ++u) {
             const int o = e + u * es;
             const VT val = __shfl_sync(FULL, cv, gbase + o);
             const int col = __shfl_sync(FULL, cc, gbase + o);
@@ -94,8 +97,8 @@ constexpr int COOP_MINB = 4;
 // elements in flight per lane
 template <int KPL> constexpr int group_unroll() { return KPL == 1 ? 4 : (KPL == 2 ? 2 : 1); }
 
-template <int KPL, typename VT, bool COOP>
-__global__ void __launch_bounds__(GROUP_THREADS, COOP ? COOP_MINB : group_minb<KPL>())
+template <int KPL, typename VT, int KCT>
+__global__ void __launch_bounds__(GROUP_THREADS, KCT ? COOP_MINB : group_minb<KPL>())
 csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                  const VT *__restrict__ v, const VT *__restrict__ X, long long ldx,
                  double *__restrict__ Y, long long ldy, int m, int k, int gl_shift,
@@ -130,8 +133,8 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             }
             Acc<VT> acc[KPL];
             int j = a + e;
-            if (COOP) {
-                coop_row<KPL>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
+            if (KCT) {
+                coop_row<KPL, KCT>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
                               [&](int col, int p) {
                                   return ld_x(X + (long long)col * ldx + cl + p * kc, pl);
                               },
@@ -186,7 +189,7 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
 constexpr int WINDOW_MINB = 2;
 constexpr int WINDOW_SMEM = 100 * 1024;  // bytes of X per CTA (two CTAs per SM)
 
-template <int KPL, typename VT>
+template <int KPL, typename VT, int KCT>
 __global__ void __launch_bounds__(GROUP_THREADS, WINDOW_MINB)
 csr_window_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                   const VT *__restrict__ v, const VT *__restrict__ X, long long ldx,
@@ -279,13 +282,13 @@ csr_window_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             }
             Acc<VT> acc[KPL];
             int j = a + e;
-            if (kc > 1) {
+            if (KCT) {
                 if (staged)
-                    coop_row<KPL>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
+                    coop_row<KPL, KCT>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
                                   [&](int col, int p) { return xs[(col - cmin) * k + cl + p * kc]; },
                                   acc, pf);
                 else
-                    coop_row<KPL>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
+                    coop_row<KPL, KCT>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
                                   [&](int col, int p) {
                                       return ld_x(X + (long long)col * ldx + cl + p * kc, pl);
                                   },
@@ -342,6 +345,20 @@ int ilog2(int v) {
     return s;
 }
 
+// Calls f(std::integral_constant<int, KC>) for the column-lane count kc (1 = not cooperative).
+template <typename F>
+cudaError_t with_kc(int kc, F f) {
+    switch (kc) {
+        case 1: return f(std::integral_constant<int, 0>());
+        case 2: return f(std::integral_constant<int, 2>());
+        case 4: return f(std::integral_constant<int, 4>());
+        case 8: return f(std::integral_constant<int, 8>());
+        case 16: return f(std::integral_constant<int, 16>());
+        case 32: return f(std::integral_constant<int, 32>());
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 template <int KPL, typename VT>
 cudaError_t launch_window(const Handle &h, const VT *x, long long ldx, double *y, long long ldy,
                           int k, cudaStream_t s) {
@@ -351,58 +368,57 @@ cudaError_t launch_window(const Handle &h, const VT *x, long long ldx, double *y
     const unsigned grid = (unsigned)(ntiles < cap ? (ntiles > 0 ? ntiles : 1) : cap);
     const int max_w = (int)(WINDOW_SMEM / ((size_t)k * sizeof(VT)));
     const size_t smem = (size_t)max_w * k * sizeof(VT);
-    static const cudaError_t attr = cudaFuncSetAttribute(
-        csr_window_kernel<KPL, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WINDOW_SMEM);
-    if (attr != cudaSuccess) return attr;
-    csr_window_kernel<KPL, VT><<<grid, GROUP_THREADS, smem, s>>>(
-        h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, ilog2(h.lanes_per_row),
-        ilog2(h.col_lanes), tr, max_w);
-    return cudaGetLastError();
+    return with_kc(h.col_lanes, [&](auto KCC) {
+        constexpr int KCT = decltype(KCC)::value;
+        static const cudaError_t attr = cudaFuncSetAttribute(
+            csr_window_kernel<KPL, VT, KCT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            WINDOW_SMEM);
+        if (attr != cudaSuccess) return attr;
+        csr_window_kernel<KPL, VT, KCT><<<grid, GROUP_THREADS, smem, s>>>(
+            h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, ilog2(h.lanes_per_row),
+            ilog2(h.col_lanes), tr, max_w);
+        return cudaGetLastError();
+    });
+}
+
+template <int KPL, typename VT>
+cudaError_t launch_rows(const Handle &h, const VT *x, long long ldx, double *y, long long ldy,
+                        int k, cudaStream_t s) {
+    const int kc = h.col_lanes;
+    const int tr = h.rows_per_tile;
+    const long long ntiles = ((long long)h.m + tr - 1) / tr;
+    const long long want = (ntiles + (GROUP_THREADS / 32) - 1) / (GROUP_THREADS / 32);
+    const int minb = kc > 1 ? COOP_MINB : group_minb<KPL>();
+    const long long cap = (long long)h.sm_count * minb;
+    const unsigned grid = (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
+    const int gs = ilog2(h.lanes_per_row), ks = ilog2(kc);
+    return with_kc(kc, [&](auto KCC) {
+        constexpr int KCT = decltype(KCC)::value;
+        csr_group_kernel<KPL, VT, KCT><<<grid, GROUP_THREADS, 0, s>>>(
+            h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, gs, ks, tr);
+        return cudaGetLastError();
+    });
 }
 
 template <typename VT>
 cudaError_t launch_group(const Handle &h, const void *X, long long ldx, void *Y, long long ldy,
                          int k, cudaStream_t s) {
-    const int gl = h.lanes_per_row, kc = h.col_lanes, kpl = h.cols_per_lane;
+    const VT *x = (const VT *)X;
+    double *y = (double *)Y;
     if (h.x_window) {
-        const VT *x = (const VT *)X;
-        double *y = (double *)Y;
-        switch (kpl) {
+        switch (h.cols_per_lane) {
             case 1: return launch_window<1, VT>(h, x, ldx, y, ldy, k, s);
             case 2: return launch_window<2, VT>(h, x, ldx, y, ldy, k, s);
             case 4: return launch_window<4, VT>(h, x, ldx, y, ldy, k, s);
             default: return cudaErrorInvalidValue;
         }
     }
-    const int gpw = 32 / gl;
-    const int tr = h.rows_per_tile;
-    const long long ntiles = ((long long)h.m + tr - 1) / tr;
-    const long long want = (ntiles + (GROUP_THREADS / 32) - 1) / (GROUP_THREADS / 32);
-    const int minb = kc > 1 ? COOP_MINB
-                            : (kpl == 1 ? group_minb<1>() : (kpl == 2 ? group_minb<2>() : group_minb<4>()));
-    const long long cap = (long long)h.sm_count * minb;
-    const unsigned grid = (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
-    (void)gpw;
-    const int gs = ilog2(gl), ks = ilog2(kc);
-    const VT *x = (const VT *)X;
-    const VT *v = (const VT *)h.v;
-    double *y = (double *)Y;
-    const bool coop = kc > 1;
-#define PAVA_GROUP_LAUNCH(KPLV)                                                               \
-    if (coop)                                                                                 \
-        csr_group_kernel<KPLV, VT, true><<<grid, GROUP_THREADS, 0, s>>>(                      \
-            h.rp, h.ci, v, x, ldx, y, ldy, h.m, k, gs, ks, tr);                               \
-    else                                                                                      \
-        csr_group_kernel<KPLV, VT, false><<<grid, GROUP_THREADS, 0, s>>>(                     \
-            h.rp, h.ci, v, x, ldx, y, ldy, h.m, k, gs, ks, tr);
-    switch (kpl) {
-        case 1: PAVA_GROUP_LAUNCH(1) break;
-        case 2: PAVA_GROUP_LAUNCH(2) break;
-        case 4: PAVA_GROUP_LAUNCH(4) break;
+    switch (h.cols_per_lane) {
+        case 1: return launch_rows<1, VT>(h, x, ldx, y, ldy, k, s);
+        case 2: return launch_rows<2, VT>(h, x, ldx, y, ldy, k, s);
+        case 4: return launch_rows<4, VT>(h, x, ldx, y, ldy, k, s);
         default: return cudaErrorInvalidValue;
     }
-#undef PAVA_GROUP_LAUNCH
-    return cudaGetLastError();
 }
 
 __global__ void narrow_kernel(const double *__restrict__ src, float *__restrict__ dst,
