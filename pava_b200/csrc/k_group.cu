@@ -141,35 +141,31 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                               acc, pf);
                 j = b;
             }
-            // U elements at a time: all value and column loads first, then all gathers, so
-            // U memory round trips overlap instead of running one after another
-            for (; j + (U - 1) * es < b; j += U * es) {
+            // U elements at a time (the last batch predicated): all value and column loads
+            // first, then all gathers, so up to U memory round trips overlap even on short rows
+            for (; j < b; j += U * es) {
                 VT val[U];
                 int col[U];
+                bool in[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
-                    val[u] = ld_val(v + j + u * es, pf);
-                    col[u] = ld_col(ci + j + u * es, pf);
+                    in[u] = j + u * es < b;
+                    val[u] = in[u] ? ld_val(v + j + u * es, pf) : VT(0);
+                    col[u] = in[u] ? ld_col(ci + j + u * es, pf) : 0;
                 }
                 VT xv[U][KPL];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const VT *xr = X + (long long)col[u] * ldx + cl;
 #pragma unroll
-                    for (int p = 0; p < KPL; ++p) xv[u][p] = colok[p] ? ld_x(xr + p * kc, pl) : VT(0);
+                    for (int p = 0; p < KPL; ++p)
+                        xv[u][p] = in[u] && colok[p] ? ld_x(xr + p * kc, pl) : VT(0);
                 }
 #pragma unroll
                 for (int u = 0; u < U; ++u)
 #pragma unroll
                     for (int p = 0; p < KPL; ++p)
-                        if (colok[p]) acc[p].add(val[u], xv[u][p]);
-            }
-            for (; j < b; j += es) {
-                const VT val = ld_val(v + j, pf);
-                const VT *xr = X + (long long)ld_col(ci + j, pf) * ldx + cl;
-#pragma unroll
-                for (int p = 0; p < KPL; ++p)
-                    if (colok[p]) acc[p].add(val, ld_x(xr + p * kc, pl));
+                        if (in[u] && colok[p]) acc[p].add(val[u], xv[u][p]);
             }
 #pragma unroll
             for (int p = 0; p < KPL; ++p) {
