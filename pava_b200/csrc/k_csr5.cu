@@ -147,6 +147,7 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
         const long long t0 = c * G;
         const VT *vb = vals + t0 * 32 * SIGMA;
         const IT *cb = cols + t0 * 32 * SIGMA;
+        const VT *xb = x + (sizeof(IT) == 2 ? r_first : 0);  // base of the column offsets
         const int NB = G * NBT;
 
         CBlk<IT> c1 = CBlk<IT>::load(cb, 1, lane, pf);
@@ -156,7 +157,7 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
         {
             const CBlk<IT> c0 = CBlk<IT>::load(cb, 0, lane, pf);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) x0[q] = gather_x(x, c0.col(q, r_first), pl);
+            for (int q = 0; q < 4; ++q) x0[q] = c0.gather(q, xb, pl);
         }
         unsigned Fn = ld_stream(desc + t0 * 32 + lane, pf);
         int rsn = tile_ptr[t0];
@@ -179,7 +180,7 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
             VT x1[4];
             if (blk + 1 < NB) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) x1[q] = gather_x(x, c1.col(q, r_first), pl);
+                for (int q = 0; q < 4; ++q) x1[q] = c1.gather(q, xb, pl);
             }
             const int qb = blk % NBT;
             if (qb == 0) {  // tile start

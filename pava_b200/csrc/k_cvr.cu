@@ -248,6 +248,7 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
         const int i_t = M->i_t;
         const VT *vb = vals + c * L;
         const IT *cb = cols + c * L;
+        const VT *xb = x + (sizeof(IT) == 2 ? r_first : 0);  // base of the column offsets
         const unsigned *fb = flags + c * S;
         auto LF = [&](int b) { return ld_flag(fb + ((4 * b) >> 5) * 32 + lane); };
 
@@ -265,7 +266,7 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
         {
             const CBlk<IT> c0 = CBlk<IT>::load(cb, 0, lane, pf);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) x0[q] = gather_x(x, c0.col(q, r_first), pl);
+            for (int q = 0; q < 4; ++q) x0[q] = c0.gather(q, xb, pl);
         }
 #pragma unroll 1
         for (int blk = 0; blk < NB; ++blk) {
@@ -280,7 +281,7 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
             VT x1[4];
             if (blk + 1 < NB) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) x1[q] = gather_x(x, c1.col(q, r_first), pl);
+                for (int q = 0; q < 4; ++q) x1[q] = c1.gather(q, xb, pl);
             }
             const unsigned fw = f0;
 #pragma unroll

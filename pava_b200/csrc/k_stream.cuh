@@ -47,6 +47,12 @@ template <> struct VBlk<float> {
 
 template <typename IT> struct CBlk;
 template <> struct CBlk<int> {
+    // x of element q: xb is x itself for 32-bit columns; column -1 reads nothing, gives 0
+    template <typename T>
+    __device__ __forceinline__ T gather(int q, const T *xb, uint64_t pol) const {
+        const int c = col(q, 0);
+        return c >= 0 ? ld_x(xb + c, pol) : T(0);
+    }
     int4 a;
     __device__ __forceinline__ int col(int q, int) const {
         return q == 0 ? a.x : q == 1 ? a.y : q == 2 ? a.z : a.w;
@@ -58,6 +64,13 @@ template <> struct CBlk<int> {
     }
 };
 template <> struct CBlk<short> {
+    // x of element q: xb = x + (the chunk's first row); the offset DELTA_NONE reads nothing
+    template <typename T>
+    __device__ __forceinline__ T gather(int q, const T *xb, uint64_t pol) const {
+        const unsigned w = q < 2 ? a.x : a.y;
+        const int d = (q & 1) ? ((int)w >> 16) : ((int)(w << 16) >> 16);
+        return d != DELTA_NONE ? ld_x(xb + d, pol) : T(0);
+    }
     uint2 a;
     __device__ __forceinline__ int col(int q, int r_first) const {
         const unsigned w = q < 2 ? a.x : a.y;

@@ -2,6 +2,8 @@
 // shared by the CVR and CSR5 forms.
 
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
 
 #include "pava_internal.h"
 
@@ -88,9 +90,7 @@ cudaError_t build_augmented_rowptr(const int *rp, int m, long long padded_total,
     int *empties = nullptr;
     cudaError_t e = cudaMallocAsync(&empties, sizeof(int) * ((size_t)m + 1), s);
     if (e != cudaSuccess) return e;
-    cub::CountingInputIterator<int> rows(0);
-    cub::TransformInputIterator<int, EmptyRow, cub::CountingInputIterator<int>> flags(
-        rows, EmptyRow{rp});
+    auto flags = thrust::make_transform_iterator(thrust::make_counting_iterator(0), EmptyRow{rp});
     // empties[0] = 0, empties[1..m] = inclusive scan of flag(0..m-1)
     size_t tmp_bytes = 0;
     cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, flags, empties + 1, m, s);
