@@ -47,7 +47,9 @@ template <> struct VBlk<float> {
 
 template <typename IT> struct CBlk;
 template <> struct CBlk<int> {
-    // x of element q: xb is x itself for 32-bit columns; column -1 reads nothing, gives 0
+    // x of element q: xb is x itself for 32-bit columns.  Column -1 (the dummy element of an
+    // empty row, or chunk padding) reads nothing and gives 0, so a non-finite x never leaks
+    // into an empty row.
     template <typename T>
     __device__ __forceinline__ T gather(int q, const T *xb, uint64_t pol) const {
         const int c = col(q, 0);

@@ -69,13 +69,6 @@ __device__ __forceinline__ float ld_x(const float *p, uint64_t pol) {
     return r;
 }
 
-// Gathers x[c]; the sentinel column -1 (dummy elements of empty rows and of chunk padding)
-// reads nothing and yields 0, so a non-finite x can never leak into an empty row.
-template <typename T>
-__device__ __forceinline__ T gather_x(const T *x, int c, uint64_t pol) {
-    return c >= 0 ? ld_x(x + c, pol) : T(0);
-}
-
 // Last index r in [0, n) with a[r] <= key (a sorted ascending, a[0] <= key).
 __device__ __forceinline__ int upper_bound_m1(const int *a, int n, long long key) {
     int lo = 0, hi = n;  // first index with a[idx] > key lies in [lo, hi]
