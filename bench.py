@@ -311,22 +311,26 @@ def main():
     den = np.maximum(np.maximum(np.abs(ypn), absum), 1e-300)
     max_rel_vs_plain = float(np.max(np.abs(yc - ypn) / den))
 
-    # end-to-end through the public host-buffer entry point: H2D x, SpMV, D2H y per step
+    # end-to-end through the public host-buffer entry point: every step copies x in from pinned
+    # host memory, runs the SpMV and copies y out (pava_spmv_host_async: consecutive steps
+    # overlap one step's copy-in, another's SpMV and a third's copy-out)
     xh = torch.from_numpy(x_host).pin_memory()
     yh = torch.empty(A.m, dtype=torch.float64).pin_memory()
     KE = max(3, min(K, 20))
     for _ in range(2):
-        mat.spmv_host(xh, yh, stream=stream)
+        mat.spmv_host_async(xh, yh, stream=stream)
+    mat.wait()
     barrier()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
     ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ea.record(stream)
     for _ in range(KE):
-        mat.spmv_host(xh, yh, stream=stream)
+        mat.spmv_host_async(xh, yh, stream=stream)
     eb.record(stream)
     eb.synchronize()
+    mat.wait()
     e2e_ms = ea.elapsed_time(eb) / KE
+    e2e_ok = bool(np.array_equal(yh.numpy(), yc))
     e2e_ms, = max_over_ranks([e2e_ms], world, dev)
 
     peak, peak_kind = peak_hbm()
@@ -369,7 +373,8 @@ def main():
                          "kernel": kernel_key, "kernel_ms": round(main_ms, 6)},
             "e2e": {"value": round(aggregate_gbps(world, alg, e2e_ms), 3), "unit": "GB/s",
                     "ms_per_step": round(e2e_ms, 6), "h2d_bytes_per_step": 8 * A.n,
-                    "d2h_bytes_per_step": 8 * A.m},
+                    "d2h_bytes_per_step": 8 * A.m, "entry_point": "pava_spmv_host_async",
+                    "y_equals_device_result": e2e_ok},
             "gpu_launches": 2 * K,
             "clocks": clocks.summary(),
             "format_bytes_per_step": info["format_bytes"],

@@ -139,6 +139,17 @@ pava_status pava_spmv_stage(pava_handle *h, const void *x, void *y, void *stream
  * the handle after the first call. */
 pava_status pava_spmv_host(pava_handle *h, const void *x_host, void *y_host, void *stream);
 
+/* Pipelined form of pava_spmv_host: queues the copy of x in, the SpMV and the copy of y out on
+ * the handle's own streams and returns at once, so that consecutive calls overlap one call's
+ * copy-in, another's SpMV and a third's copy-out (two staging slots).  `stream` waits for the
+ * call's copy-out.  The copy-in does not wait for `stream`: x_host must hold its values when
+ * the call is made.  x_host and y_host should be pinned, and must stay untouched until the call
+ * is complete: after pava_spmv_host_wait, or once `stream` has reached the point of the call.
+ * No counterpart in the reference. */
+pava_status pava_spmv_host_async(pava_handle *h, const void *x_host, void *y_host,
+                                 void *stream);
+/* Waits until every pava_spmv_host_async call on the handle is complete. */
+pava_status pava_spmv_host_wait(pava_handle *h);
 pava_status pava_get_info(const pava_handle *h, pava_info *out);
 
 /* anonymouslibHandle::destroy / asCSR (csr5/anonymouslib_avx512.h:80-104,258-262). */

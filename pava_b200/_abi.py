@@ -85,6 +85,8 @@ GPU_SYMBOLS = [
     ("pava_spmv_stage", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     ("pava_spmm", c_int, [c_void_p, c_int, c_void_p, c_ll, c_void_p, c_ll, c_void_p]),
     ("pava_spmv_host", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("pava_spmv_host_async", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("pava_spmv_host_wait", c_int, [c_void_p]),
     ("pava_get_info", c_int, [c_void_p, ctypes.POINTER(PavaInfo)]),
     ("pava_destroy", c_int, [c_void_p]),
     ("pava_last_error", c_char_p, []),

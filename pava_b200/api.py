@@ -129,6 +129,18 @@ class SpMatrix:
         _abi.check(_abi.gpu().pava_spmv_host(self._h, xp, yp, _abi.c_void_p(sp)))
         return y
 
+    def spmv_host_async(self, x, y, stream=None):
+        """Pipelined end-to-end SpMV on pinned host tensors (pava_spmv_host_async): returns at
+        once; consecutive calls overlap their copies and SpMVs.  x and y must stay untouched
+        until wait() (or until `stream` reaches the call)."""
+        sp = _stream_ptr(stream) if stream is not None else None
+        _abi.check(_abi.gpu().pava_spmv_host_async(self._h, x.data_ptr(), y.data_ptr(),
+                                                   _abi.c_void_p(sp)))
+        return y
+
+    def wait(self):
+        _abi.check(_abi.gpu().pava_spmv_host_wait(self._h))
+
     def close(self):
         if getattr(self, "_h", None):
             _abi.gpu().pava_destroy(self._h)

@@ -9,11 +9,58 @@
 
 #include "pava_internal.h"
 
+// Pipeline of the asynchronous host-buffer entry point: two staging slots, one stream each for
+// copies in, SpMVs and copies out, and per-slot events that order the reuse of a slot.
+struct HostPipe {
+    bool ready = false;
+    cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr},
+                ev_out[2] = {nullptr, nullptr};
+    void *x[2] = {nullptr, nullptr}, *y[2] = {nullptr, nullptr};
+    unsigned long long calls = 0;
+};
+
 struct pava_handle {
     pava::Handle h;
     void *x_dev = nullptr;  // buffers of the host-buffer entry point
     void *y_dev = nullptr;
+    HostPipe pipe;
 };
+
+namespace {
+
+void free_pipe(HostPipe &p) {
+    if (p.out) cudaStreamSynchronize(p.out);
+    for (int k = 0; k < 2; ++k) {
+        if (p.ev_in[k]) cudaEventDestroy(p.ev_in[k]);
+        if (p.ev_comp[k]) cudaEventDestroy(p.ev_comp[k]);
+        if (p.ev_out[k]) cudaEventDestroy(p.ev_out[k]);
+        cudaFree(p.x[k]);
+        cudaFree(p.y[k]);
+    }
+    if (p.in) cudaStreamDestroy(p.in);
+    if (p.comp) cudaStreamDestroy(p.comp);
+    if (p.out) cudaStreamDestroy(p.out);
+    p = HostPipe();
+}
+
+cudaError_t make_pipe(HostPipe &p, size_t sx, size_t sy) {
+    cudaError_t e = cudaStreamCreateWithFlags(&p.in, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p.comp, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p.out, cudaStreamNonBlocking);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        e = cudaEventCreateWithFlags(&p.ev_in[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.ev_comp[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.ev_out[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaMalloc(&p.x[k], sx);
+        if (e == cudaSuccess) e = cudaMalloc(&p.y[k], sy);
+    }
+    if (e != cudaSuccess) free_pipe(p);
+    else p.ready = true;
+    return e;
+}
+
+}  // namespace
 
 namespace {
 
@@ -451,6 +498,43 @@ pava_status pava_spmv_host(pava_handle *H, const void *x_host, void *y_host, voi
     return PAVA_SUCCESS;
 }
 
+pava_status pava_spmv_host_async(pava_handle *H, const void *x_host, void *y_host,
+                                 void *stream) {
+    if (!H) return fail(PAVA_E_INVALID_ARG, "handle is NULL");
+    pava::Handle &h = H->h;
+    if (!x_host || !y_host) return fail(PAVA_E_INVALID_ARG, "x or y is NULL");
+    const size_t sx = value_bytes(h.precision) * (size_t)(h.n ? h.n : 1);
+    const size_t sy = sizeof(double) * (size_t)(h.m ? h.m : 1);
+    HostPipe &p = H->pipe;
+    if (!p.ready) PAVA_CUDA(make_pipe(p, sx, sy), "host pipeline set-up");
+    const int k = (int)(p.calls & 1);
+    cudaStream_t s = (cudaStream_t)stream;
+    // copy in: after the SpMV that last read this slot (not after the caller's stream, which
+    // waits for earlier calls' copies out: x_host must be ready when the call is made)
+    if (p.calls >= 2) PAVA_CUDA(cudaStreamWaitEvent(p.in, p.ev_comp[k], 0), "cudaStreamWaitEvent");
+    PAVA_CUDA(cudaMemcpyAsync(p.x[k], x_host, sx, cudaMemcpyHostToDevice, p.in), "copy x");
+    PAVA_CUDA(cudaEventRecord(p.ev_in[k], p.in), "cudaEventRecord");
+    // SpMV: after its x arrived and after the copy-out that last read this slot's y
+    PAVA_CUDA(cudaStreamWaitEvent(p.comp, p.ev_in[k], 0), "cudaStreamWaitEvent");
+    if (p.calls >= 2) PAVA_CUDA(cudaStreamWaitEvent(p.comp, p.ev_out[k], 0), "cudaStreamWaitEvent");
+    pava_status st = pava_spmv(H, p.x[k], p.y[k], p.comp);
+    if (st != PAVA_SUCCESS) return st;
+    PAVA_CUDA(cudaEventRecord(p.ev_comp[k], p.comp), "cudaEventRecord");
+    // copy out, and the caller's stream waits for it
+    PAVA_CUDA(cudaStreamWaitEvent(p.out, p.ev_comp[k], 0), "cudaStreamWaitEvent");
+    PAVA_CUDA(cudaMemcpyAsync(y_host, p.y[k], sy, cudaMemcpyDeviceToHost, p.out), "copy y");
+    PAVA_CUDA(cudaEventRecord(p.ev_out[k], p.out), "cudaEventRecord");
+    PAVA_CUDA(cudaStreamWaitEvent(s, p.ev_out[k], 0), "cudaStreamWaitEvent");
+    ++p.calls;
+    return PAVA_SUCCESS;
+}
+
+pava_status pava_spmv_host_wait(pava_handle *H) {
+    if (!H) return fail(PAVA_E_INVALID_ARG, "handle is NULL");
+    if (H->pipe.ready) PAVA_CUDA(cudaStreamSynchronize(H->pipe.out), "cudaStreamSynchronize");
+    return PAVA_SUCCESS;
+}
+
 pava_status pava_get_info(const pava_handle *H, pava_info *out) {
     if (!H || !out) return fail(PAVA_E_INVALID_ARG, "NULL argument");
     const pava::Handle &h = H->h;
@@ -484,6 +568,7 @@ pava_status pava_get_info(const pava_handle *H, pava_info *out) {
 
 pava_status pava_destroy(pava_handle *H) {
     if (!H) return PAVA_SUCCESS;
+    free_pipe(H->pipe);
     free_handle_buffers(H->h);
     cudaFree(H->x_dev);
     cudaFree(H->y_dev);
