@@ -362,6 +362,10 @@ def main():
                        "alg_bytes_per_step": alg},
             "pct_of_hbm_peak": round(100.0 * alg / (ms * 1e-3) / 1e9 / peak, 2),
             "pct_of_8tbs_nominal": round(100.0 * alg / (ms * 1e-3) / 1e9 / 8000.0, 2),
+            # the reference's CSR5 byte model (csr5/detail/utils.h getB: x counted per nonzero),
+            # for comparison with the GB/s the reference prints
+            "csr5_getB_GBps": round(((A.m + 1 + A.nnz) * 4.0 + (2.0 * A.nnz + A.m) * 8.0)
+                                    / (ms * 1e-3) / 1e9, 3),
             "plain_fp64": {"format": "csr", "ms": round(plain_ms, 6),
                            "GB/s": round(alg / (plain_ms * 1e-3) / 1e9, 3)},
             "variants": {k: {"ms": round(v["ms"], 6), "GB/s": round(alg / (v["ms"] * 1e-3) / 1e9, 3),

@@ -68,9 +68,11 @@ typedef struct pava_csr {
 
 /* Tuning knobs; zero means "default". */
 typedef struct pava_opts {
-    int steps;            /* CVR: steps per warp chunk, a multiple of 32 (default 64) */
-    int sigma;            /* CSR5: elements per lane per tile, multiple of 4, <= 32 (default 16) */
-    int tiles_per_chunk;  /* CSR5: tiles per warp chunk (default 4) */
+    int steps;            /* CVR: steps per warp chunk, 32, 64 or 128 (default 64; 32 when a
+                             matrix gives fewer than 24 chunks of 64 steps per SM) */
+    int sigma;            /* CSR5: elements per lane per tile, 8, 12, 16, 24 or 32 (default 16) */
+    int tiles_per_chunk;  /* CSR5: tiles per warp chunk, 1 .. 64 (default 4; 2 or 1 when a
+                             matrix gives fewer than 4 x 24 tiles per SM) */
     int precision;        /* pava_precision */
     int index_mode;       /* pava_index_mode */
     int lanes_per_row;    /* CSR: lanes per row group, 1, 2, 4, 8, 16 or 32 (default: from

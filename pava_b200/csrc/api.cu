@@ -323,8 +323,17 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
     h.m = A->m;
     h.n = A->n;
     h.nnz = A->nnz;
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&h.sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (ce != cudaSuccess) { delete H; return fail_cuda(ce, "no usable CUDA device"); }
+    h.device = dev;
+    // default chunk sizes: the larger forms unless that leaves fewer than ~24 warp chunks per
+    // SM (small matrices), where shorter chunks keep every SM busy
+    const long long want_chunks = 24LL * h.sm_count;
     if (format == PAVA_FORMAT_CVR) {
-        h.S = o.steps ? o.steps : 64;
+        h.S = o.steps ? o.steps : ((long long)h.nnz / (32 * 64) < want_chunks ? 32 : 64);
         if (h.S != 32 && h.S != 64 && h.S != 128) {
             delete H;
             return fail(PAVA_E_UNSUPPORTED_PARAMS, "CVR steps must be 32, 64 or 128");
@@ -332,7 +341,12 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
         h.L = 32LL * h.S;
     } else if (format == PAVA_FORMAT_CSR5) {
         h.sigma = o.sigma ? o.sigma : 16;
-        h.G = o.tiles_per_chunk ? o.tiles_per_chunk : 4;
+        if (o.tiles_per_chunk) {
+            h.G = o.tiles_per_chunk;
+        } else {  // 4 tiles per chunk, fewer for small matrices
+            const long long tiles = (long long)h.nnz / (32LL * h.sigma);
+            h.G = tiles >= 4 * want_chunks ? 4 : (tiles >= 2 * want_chunks ? 2 : 1);
+        }
         if (!(h.sigma == 8 || h.sigma == 12 || h.sigma == 16 || h.sigma == 24 || h.sigma == 32) ||
             h.G < 1 || h.G > 64) {
             delete H;
@@ -361,12 +375,6 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
                                     : why);
         }
     }
-    cudaStream_t s = (cudaStream_t)stream;
-    int dev = 0;
-    cudaError_t ce = cudaGetDevice(&dev);
-    if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&h.sm_count, cudaDevAttrMultiProcessorCount, dev);
-    if (ce != cudaSuccess) { delete H; return fail_cuda(ce, "no usable CUDA device"); }
-    h.device = dev;
 
     // inputs on the device
     const int *rp = A->row_ptr, *ci = A->col_idx;

@@ -58,6 +58,8 @@ def main():
     p.add_argument("--variants", default="cvr:steps=128")
     p.add_argument("--reps", type=int, default=3)
     p.add_argument("--quiet", action="store_true")
+    p.add_argument("--flush", action="store_true",
+                   help="write a 512 MB buffer between timed reps (matrices smaller than L2)")
     a = p.parse_args()
 
     import torch
@@ -83,7 +85,10 @@ def main():
         s = torch.cuda.current_stream().cuda_stream
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(a.reps)]
+        scratch = torch.empty(64 << 20, dtype=torch.float64, device="cuda") if a.flush else None
         for k in range(a.reps):
+            if scratch is not None:
+                scratch.fill_(float(k))  # evicts the matrix and x from the 126 MB L2
             ev[k][0].record()
             mat.spmv_raw(x.data_ptr(), y.data_ptr(), s, 1)
             ev[k][1].record()
