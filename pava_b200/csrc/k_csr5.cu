@@ -129,6 +129,8 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
                  double *__restrict__ y, double *__restrict__ carry_head,
                  double *__restrict__ carry_tail, long long nchunks, int G, int m) {
     constexpr int NBT = SIGMA / 4;  // blocks per tile
+    // the carry fixup that follows may launch now; it waits for this grid to finish
+    asm volatile("griddepcontrol.launch_dependents;");
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
     const long long nwarps = (long long)gridDim.x * SPMV_WARPS;

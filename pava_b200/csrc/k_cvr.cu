@@ -238,6 +238,8 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
     const unsigned lt = lanemask_lt();
+    // the carry fixup that follows may launch now; it waits for this grid to finish
+    asm volatile("griddepcontrol.launch_dependents;");
     const long long nwarps = (long long)gridDim.x * SPMV_WARPS;
 
     for (long long c = (long long)blockIdx.x * SPMV_WARPS + w; c < nchunks; c += nwarps) {

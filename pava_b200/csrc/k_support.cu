@@ -52,6 +52,9 @@ __global__ void carry_fixup_kernel(const char *__restrict__ meta, size_t stride,
                                    const double *__restrict__ carry_head,
                                    const double *__restrict__ carry_tail, double *__restrict__ y,
                                    long long nchunks, int m) {
+    // launched as a programmatic dependent of the SpMV kernel: wait until that grid has
+    // finished and its carries are visible (returns at once for an ordinary launch)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int lane = threadIdx.x & 31;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long c1 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c1 < nchunks;
@@ -112,10 +115,21 @@ cudaError_t carry_fixup(const Handle &h, void *y, cudaStream_t s) {
     long long blocks = (h.nchunks * 32 + 255) / 256;
     const long long cap = (long long)h.sm_count * 16;
     if (blocks > cap) blocks = cap;
-    carry_fixup_kernel<<<(unsigned)blocks, 256, 0, s>>>((const char *)h.meta, h.meta_stride,
-                                                        h.arp, h.L, h.carry_head, h.carry_tail,
-                                                        (double *)y, h.nchunks, h.m);
-    return cudaGetLastError();
+    // programmatic dependent launch: the fixup grid is launched while the SpMV grid runs (its
+    // launch latency hidden) and waits for it in griddepcontrol.wait
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, carry_fixup_kernel, (const char *)h.meta, h.meta_stride,
+                              (const int *)h.arp, h.L, (const double *)h.carry_head,
+                              (const double *)h.carry_tail, (double *)y, h.nchunks, h.m);
 }
 
 }  // namespace pava
