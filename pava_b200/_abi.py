@@ -35,7 +35,7 @@ E_TOO_LARGE = -15
 
 FORMAT_CSR, FORMAT_CSR5, FORMAT_CVR = 0, 1, 3
 PREC_FP64, PREC_FP32C = 0, 1
-INDEX_I32, INDEX_DELTA16 = 0, 1
+INDEX_I32, INDEX_DELTA16, INDEX_AUTO = 0, 1, 2
 
 
 class PavaCsr(ctypes.Structure):

@@ -230,6 +230,7 @@ pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double 
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         cudaFreeAsync(d_ovf, s);
         if (e != cudaSuccess) return fail_cuda(e, "conversion");
+        h.d16_overflow = ovf ? 1 : 0;
         if (ovf)
             return fail(PAVA_E_UNSUPPORTED_PARAMS,
                         "16-bit column offsets: a column lies more than 32767 from its chunk's first row");
@@ -309,10 +310,14 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
     if (opts) o = *opts;
     if (o.precision != PAVA_PREC_FP64 && o.precision != PAVA_PREC_FP32C)
         return fail(PAVA_E_UNSUPPORTED_VALUE_TYPE, "unknown precision");
-    if (o.index_mode != PAVA_INDEX_I32 && o.index_mode != PAVA_INDEX_DELTA16)
+    if (o.index_mode != PAVA_INDEX_I32 && o.index_mode != PAVA_INDEX_DELTA16 &&
+        o.index_mode != PAVA_INDEX_AUTO)
         return fail(PAVA_E_UNSUPPORTED_PARAMS, "unknown index mode");
+    if (format == PAVA_FORMAT_CSR && o.index_mode == PAVA_INDEX_AUTO) o.index_mode = PAVA_INDEX_I32;
     if (format == PAVA_FORMAT_CSR && o.index_mode != PAVA_INDEX_I32)
         return fail(PAVA_E_UNSUPPORTED_PARAMS, "the plain CSR form takes 32-bit columns");
+    const bool auto_index = o.index_mode == PAVA_INDEX_AUTO;
+    if (auto_index) o.index_mode = PAVA_INDEX_DELTA16;  // tried first
 
     pava_handle *H = new (std::nothrow) pava_handle();
     if (!H) return fail(PAVA_E_NOMEM, "host allocation failed");
@@ -420,6 +425,13 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
     st = convert(h, rp, ci, v, s);
+    if (st == PAVA_E_UNSUPPORTED_PARAMS && auto_index && h.d16_overflow) {
+        // a column does not fit 16 bits: convert again with 32-bit columns
+        free_handle_buffers(h);
+        h.device_bytes = 0;
+        h.index_mode = PAVA_INDEX_I32;
+        st = convert(h, rp, ci, v, s);
+    }
     if (st == PAVA_SUCCESS) {
         cudaEventRecord(e1, s);
         ce = cudaEventSynchronize(e1);
@@ -594,7 +606,10 @@ int conduct_gpu(int format, int m, int n, int nnz, const int *rp, const int *ci,
                 const double *v, const double *x, double *y, const char *name, int iters) {
     pava_csr A{m, n, nnz, rp, ci, v, 0};
     pava_handle *H = nullptr;
-    int st = pava_create(&A, format, nullptr, nullptr, &H);
+    pava_opts o;
+    memset(&o, 0, sizeof(o));
+    o.index_mode = PAVA_INDEX_AUTO;  // 16-bit column offsets where they fit: same results
+    int st = pava_create(&A, format, &o, nullptr, &H);
     if (st != PAVA_SUCCESS) {
         printf(" Performance %s %s %d %f %f \n", name ? name : "", format == PAVA_FORMAT_CVR ? "CVR" : "CSR5", 0, -1.0, -1.0);
         return st;

@@ -60,6 +60,7 @@ struct Handle {
 
     double convert_ms = 0.0;
     size_t device_bytes = 0;
+    int d16_overflow = 0;    // the last conversion found a column outside the 16-bit range
 };
 
 // Sets the message pava_last_error() returns on this thread.

@@ -92,3 +92,18 @@ def test_config3_full_size_fp32c_vs_fp64(cuda):
         bad, mx, mean = O.rel_error(y32, yr, ab, TOL32)
         assert bad == 0, (fmt, mx, mean)
         del m32
+
+
+@pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
+def test_index_auto_picks_16_bit_where_it_fits(cuda, fmt, kw):
+    """PAVA_INDEX_AUTO: 16-bit offsets on a stencil, 32-bit columns when a column is out of
+    reach; results bitwise equal to the 32-bit form either way."""
+    torch = cuda
+    for A, want in ((M.stencil27(30, seed=9), _abi.INDEX_DELTA16),
+                    (M.powerlaw(300_000, mean=12.0, seed=10), _abi.INDEX_I32)):
+        x = torch.from_numpy(M.uniform(A.n, seed=11)).cuda()
+        auto = SpMatrix(A, fmt, index_mode=_abi.INDEX_AUTO, **kw)
+        assert auto.info()["index_mode"] == want
+        y_auto = auto.spmv(x).cpu().numpy()
+        y_i32 = SpMatrix(A, fmt, index_mode=_abi.INDEX_I32, **kw).spmv(x).cpu().numpy()
+        assert np.array_equal(y_auto, y_i32)
