@@ -14,6 +14,7 @@
 // block-diagonal union of many small matrices) relies on this.
 
 #include <climits>
+#include <cstdint>
 #include <type_traits>
 
 #include "k_stream.cuh"
@@ -49,7 +50,7 @@ __device__ __forceinline__ int ld_col(const int *p, uint64_t pol) {
 // element reaches the lanes that need it by shuffle.  Slice e takes elements e, e + ES, ... in
 // ascending order, as the per-lane loop does, so the sums have the same bits.  The round count
 // is the maximum over the warp's groups so that every shuffle has all 32 lanes.
-template <int KPL, int KCT, typename VT, typename XREAD>
+template <int KPL, int KCT, int VW, typename VT, typename XREAD>
 __device__ __forceinline__ void coop_row(int a, int b, int gi, int gl, int es, int e, int kc,
                                          int lane, const int *__restrict__ ci,
                                          const VT *__restrict__ v, const bool (&colok)[KPL],
@@ -82,11 +83,34 @@ __device__ __forceinline__ void coop_row(int a, int b, int gi, int gl, int es, i
             const int col = __shfl_sync(FULL, cc, gbase + o);
             if (base + o < b) {
 #pragma unroll
-                for (int p = 0; p < KPL; ++p)
-                    if (colok[p]) acc[p].add(val, xread(col, p));
+                for (int q = 0; q < KPL / VW; ++q)
+                    if (colok[q * VW]) xread(col, q, val, acc);
             }
         }
     }
+}
+
+// Two adjacent right-hand sides of X in one 16-byte (8-byte for FP32) read.
+__device__ __forceinline__ double2 ld_x2(const double *p, uint64_t pol) {
+    double2 r;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+                 : "=d"(r.x), "=d"(r.y) : "l"(p), "l"(pol));
+    return r;
+}
+__device__ __forceinline__ float2 ld_x2(const float *p, uint64_t pol) {
+    float2 r;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+                 : "=f"(r.x), "=f"(r.y) : "l"(p), "l"(pol));
+    return r;
+}
+
+// Column of accumulator p of a lane whose first column slot is cl: VW = 1 interleaves single
+// columns across the KC lanes (cl + p KC); VW = 2 interleaves pairs (2 (cl + (p/2) KC) + p%2),
+// so that a lane reads its two columns with one vector load and a group's KC lanes read
+// 16 KC contiguous bytes.
+template <int VW>
+__device__ __forceinline__ int col_of(int cl, int p, int kc) {
+    return VW == 1 ? cl + p * kc : 2 * (cl + (p >> 1) * kc) + (p & 1);
 }
 
 constexpr int GROUP_THREADS = 256;
@@ -97,7 +121,7 @@ constexpr int COOP_MINB = 4;
 // elements in flight per lane
 template <int KPL> constexpr int group_unroll() { return KPL == 1 ? 4 : (KPL == 2 ? 2 : 1); }
 
-template <int KPL, typename VT, int KCT>
+template <int KPL, typename VT, int KCT, int VW>
 __global__ void __launch_bounds__(GROUP_THREADS, KCT ? COOP_MINB : group_minb<KPL>())
 csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                  const VT *__restrict__ v, const VT *__restrict__ X, long long ldx,
@@ -119,7 +143,18 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
 
     bool colok[KPL];
 #pragma unroll
-    for (int p = 0; p < KPL; ++p) colok[p] = cl + p * kc < k;
+    for (int p = 0; p < KPL; ++p) colok[p] = col_of<VW>(cl, p, kc) < k;
+    // reads the VW columns of slot q of X row `col` and accumulates them
+    auto xread = [&](int col, int q, VT val, Acc<VT>(&acc)[KPL]) {
+        const VT *xr = X + (long long)col * ldx + col_of<VW>(cl, q * VW, kc);
+        if (VW == 2) {
+            const auto x2 = ld_x2(xr, pl);
+            acc[2 * q].add(val, x2.x);
+            acc[2 * q + 1].add(val, x2.y);
+        } else {
+            acc[q].add(val, ld_x(xr, pl));
+        }
+    };
 
     for (long long t = (((long long)blockIdx.x * blockDim.x) + threadIdx.x) >> 5; t < ntiles;
          t += nwarps) {
@@ -134,11 +169,8 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             Acc<VT> acc[KPL];
             int j = a + e;
             if (KCT) {
-                coop_row<KPL, KCT>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
-                              [&](int col, int p) {
-                                  return ld_x(X + (long long)col * ldx + cl + p * kc, pl);
-                              },
-                              acc, pf);
+                coop_row<KPL, KCT, VW>(a, b, gi, gl, es, e, kc, lane, ci, v, colok, xread, acc,
+                                       pf);
                 j = b;
             }
             // U elements at a time (the last batch predicated): all value and column loads
@@ -153,25 +185,17 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                     val[u] = in[u] ? ld_val(v + j + u * es, pf) : VT(0);
                     col[u] = in[u] ? ld_col(ci + j + u * es, pf) : 0;
                 }
-                VT xv[U][KPL];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const VT *xr = X + (long long)col[u] * ldx + cl;
-#pragma unroll
-                    for (int p = 0; p < KPL; ++p)
-                        xv[u][p] = in[u] && colok[p] ? ld_x(xr + p * kc, pl) : VT(0);
-                }
 #pragma unroll
                 for (int u = 0; u < U; ++u)
 #pragma unroll
-                    for (int p = 0; p < KPL; ++p)
-                        if (in[u] && colok[p]) acc[p].add(val[u], xv[u][p]);
+                    for (int q = 0; q < KPL / VW; ++q)
+                        if (in[u] && colok[q * VW]) xread(col[u], q, val[u], acc);
             }
 #pragma unroll
             for (int p = 0; p < KPL; ++p) {
                 double s = acc[p].value();
                 for (int o = kc; o < gl; o <<= 1) s += __shfl_xor_sync(FULL, s, o);
-                if (valid && e == 0 && colok[p]) Y[r * ldy + cl + p * kc] = s;
+                if (valid && e == 0 && colok[p]) Y[r * ldy + col_of<VW>(cl, p, kc)] = s;
             }
         }
     }
@@ -280,15 +304,19 @@ csr_window_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             int j = a + e;
             if (KCT) {
                 if (staged)
-                    coop_row<KPL, KCT>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
-                                  [&](int col, int p) { return xs[(col - cmin) * k + cl + p * kc]; },
-                                  acc, pf);
+                    coop_row<KPL, KCT, 1>(
+                        a, b, gi, gl, es, e, kc, lane, ci, v, colok,
+                        [&](int col, int p, VT val, Acc<VT>(&ac)[KPL]) {
+                            ac[p].add(val, xs[(col - cmin) * k + cl + p * kc]);
+                        },
+                        acc, pf);
                 else
-                    coop_row<KPL, KCT>(a, b, gi, gl, es, e, kc, lane, ci, v, colok,
-                                  [&](int col, int p) {
-                                      return ld_x(X + (long long)col * ldx + cl + p * kc, pl);
-                                  },
-                                  acc, pf);
+                    coop_row<KPL, KCT, 1>(
+                        a, b, gi, gl, es, e, kc, lane, ci, v, colok,
+                        [&](int col, int p, VT val, Acc<VT>(&ac)[KPL]) {
+                            ac[p].add(val, ld_x(X + (long long)col * ldx + cl + p * kc, pl));
+                        },
+                        acc, pf);
                 j = b;
             } else if (staged) {  // WU elements' values and columns in flight, then the shared reads
                 constexpr int WU = 4;
@@ -388,10 +416,18 @@ cudaError_t launch_rows(const Handle &h, const VT *x, long long ldx, double *y, 
     const long long cap = (long long)h.sm_count * minb;
     const unsigned grid = (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
     const int gs = ilog2(h.lanes_per_row), ks = ilog2(kc);
+    // pairs of columns per vector read when every pair is whole and 2-element aligned
+    const bool vec2 = KPL >= 2 && k % 2 == 0 && ldx % 2 == 0 &&
+                      reinterpret_cast<uintptr_t>(x) % (2 * sizeof(VT)) == 0;
     return with_kc(kc, [&](auto KCC) {
         constexpr int KCT = decltype(KCC)::value;
-        csr_group_kernel<KPL, VT, KCT><<<grid, GROUP_THREADS, 0, s>>>(
-            h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, gs, ks, tr);
+        constexpr int VW2 = KPL >= 2 ? 2 : 1;
+        if (vec2)
+            csr_group_kernel<KPL, VT, KCT, VW2><<<grid, GROUP_THREADS, 0, s>>>(
+                h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, gs, ks, tr);
+        else
+            csr_group_kernel<KPL, VT, KCT, 1><<<grid, GROUP_THREADS, 0, s>>>(
+                h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, gs, ks, tr);
         return cudaGetLastError();
     });
 }
