@@ -394,7 +394,8 @@ cudaError_t launch_window(const Handle &h, const VT *x, long long ldx, double *y
     const size_t smem = (size_t)max_w * k * sizeof(VT);
     return with_kc(h.col_lanes, [&](auto KCC) {
         constexpr int KCT = decltype(KCC)::value;
-        static const cudaError_t attr = cudaFuncSetAttribute(
+        // per launch: the attribute belongs to the current device
+        const cudaError_t attr = cudaFuncSetAttribute(
             csr_window_kernel<KPL, VT, KCT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
             WINDOW_SMEM);
         if (attr != cudaSuccess) return attr;
