@@ -10,8 +10,10 @@ values with column j of row r replaced by min(r + j, n-1): the same streams, x g
 the same sectors), c3 (128^3 27-point stencil), banded (1,048,576 rows, half-bandwidth 64,
 24 per row).  ``--rows`` shrinks c2 / banded for small captures.  A variant is
 ``format:key=value;...`` with the pava_opts keys (steps, sigma, tiles_per_chunk, precision
-0=FP64 / 1=FP32C, index_mode 0=I32 / 1=DELTA16, lanes_per_row).  Prints one JSON line per
-variant with the device time of the SpMV kernel (CUDA events) unless --quiet.
+0=FP64 / 1=FP32C, index_mode 0=I32 / 1=DELTA16, lanes_per_row, col_lanes, cols_per_lane,
+rows_per_tile, x_window).  ``--k K`` (CSR variants) times pava_spmm with K right-hand sides
+instead of the SpMV.  Prints one JSON line per variant with the device time of the SpMV (or
+SpMM) kernel (CUDA events) unless --quiet.
 """
 from __future__ import annotations
 
@@ -58,6 +60,9 @@ def main():
     p.add_argument("--variants", default="cvr:steps=128")
     p.add_argument("--reps", type=int, default=3)
     p.add_argument("--quiet", action="store_true")
+    p.add_argument("--k", type=int, default=1,
+                   help="right-hand sides: k > 1 times pava_spmm on X (n x k, row-major); "
+                        "CSR variants only")
     p.add_argument("--flush", action="store_true",
                    help="write a 512 MB buffer between timed reps (matrices smaller than L2)")
     a = p.parse_args()
@@ -82,6 +87,10 @@ def main():
             print(json.dumps({"matrix": a.matrix, "format": fmt, "opts": kw, "error": str(e)}))
             continue
         y = torch.empty(A.m, dtype=torch.float64, device="cuda")
+        if a.k > 1:
+            X = torch.from_numpy(M.uniform(A.n * a.k, seed=2, fp32=True)).reshape(A.n, a.k)
+            X = X.to("cuda", x.dtype)
+            Y = torch.empty((A.m, a.k), dtype=torch.float64, device="cuda")
         s = torch.cuda.current_stream().cuda_stream
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(a.reps)]
@@ -90,9 +99,13 @@ def main():
             if scratch is not None:
                 scratch.fill_(float(k))  # evicts the matrix and x from the 126 MB L2
             ev[k][0].record()
-            mat.spmv_raw(x.data_ptr(), y.data_ptr(), s, 1)
+            if a.k > 1:
+                mat.spmm(X, Y)
+            else:
+                mat.spmv_raw(x.data_ptr(), y.data_ptr(), s, 1)
             ev[k][1].record()
-            mat.spmv_raw(x.data_ptr(), y.data_ptr(), s, 2)
+            if a.k == 1:
+                mat.spmv_raw(x.data_ptr(), y.data_ptr(), s, 2)
         torch.cuda.synchronize()
         if not a.quiet:
             info = mat.info()
@@ -100,7 +113,10 @@ def main():
             best = min(t[1:]) if len(t) > 1 else t[0]
             print(json.dumps({"matrix": a.matrix, "format": fmt, "opts": kw, "m": A.m,
                               "nnz": A.nnz, "main_ms": t, "best_ms": best,
-                              "alg_GBps": info["alg_bytes"] / (best * 1e-3) / 1e9,
+                              "k": a.k,
+                              "alg_GBps": (info["alg_bytes"]
+                                           + (a.k - 1) * (x.element_size() * A.n + 8.0 * A.m))
+                              / (best * 1e-3) / 1e9,
                               "format_GBps": info["format_bytes"] / (best * 1e-3) / 1e9,
                               "alg_bytes": info["alg_bytes"],
                               "format_bytes": info["format_bytes"],
