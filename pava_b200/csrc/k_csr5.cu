@@ -104,6 +104,36 @@ __global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long n
     hdr[c].aux = 0;
 }
 
+// Tile end: the cross-lane combine of the lanes' open row pieces.  head is the piece a lane
+// adds to the row open at its start (its whole sum when no row starts in the lane), tail the
+// sum since the lane's last row start (seen: a row starts in the lane), rowcur the row of that
+// tail, next_row the row open at the tile's end.  Rows that end in the tile go to y (or to
+// the chunk's carry slots); the open row's sum stays in carry_row / carry_val.
+__device__ __forceinline__ void tile_combine(double head, double tail, bool seen, int rowcur,
+                                             int next_row, int lane, int r_first, int r_last,
+                                             unsigned shared, long long c, double *y,
+                                             double *carry_head, double *carry_tail, int m,
+                                             int &carry_row, double &carry_val) {
+    const unsigned sm = __ballot_sync(FULL, seen);
+    const double Hs = seg_suffix(head, !seen, lane);
+    double Hn = __shfl_down_sync(FULL, Hs, 1);
+    if (lane == 31) Hn = 0.0;
+    const double H0 = __shfl_sync(FULL, Hs, 0);
+    if (sm == 0) {
+        carry_val += H0;  // the whole tile continues the open row
+    } else {
+        const int lstar = 31 - __clz(sm);
+        const double own_l = tail + Hn;
+        if (seen && lane != lstar && rowcur < m) y[rowcur] = own_l;
+        const double own = __shfl_sync(FULL, own_l, lstar);
+        if (carry_row >= 0 && lane == 0)
+            flush_row(carry_row, carry_val + H0, r_first, r_last, shared, c, y, carry_head,
+                      carry_tail, m);
+        carry_row = next_row;
+        carry_val = own;
+    }
+}
+
 #ifndef PAVA_CSR5_MINB32
 #define PAVA_CSR5_MINB32 3
 #endif
@@ -112,7 +142,8 @@ __global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long n
 #endif
 constexpr int SPMV_WARPS = 8;
 
-// CSR5 SpMV: one warp per chunk of G tiles, walked as one pipelined run of 4-step blocks
+// CSR5 SpMV (FP64 values; the FP32 form is csr5_spmv_f32_kernel below): one warp per chunk of
+// G tiles, walked as one pipelined run of 4-step blocks
 // (values two blocks ahead, columns three, x one); tile descriptors one tile ahead.
 //
 // Row ends inside a tile: when no lane of the warp starts more than KSTK rows in the tile
@@ -270,6 +301,146 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
     }
 }
 
+template <bool B> struct Flag { static constexpr bool value = B; };
+
+// CSR5 SpMV, FP32-compensated form: the same walk with a tile's sigma/4 blocks unrolled, so
+// the block pipeline rotates by register renaming instead of moves, and the fast / slow
+// choice and the tile-boundary checks are made once per tile instead of once per block.  The
+// compensated add makes this form instruction-issue bound, where the saved instructions are
+// time; the FP64 form is bandwidth bound, and unrolled it spills, so it keeps the block loop.
+template <int SIGMA, typename IT>
+__global__ void __launch_bounds__(SPMV_WARPS * 32, PAVA_CSR5_MINB32)
+csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_ptr,
+                     const unsigned *__restrict__ desc, const float *__restrict__ vals,
+                     const IT *__restrict__ cols, const float *__restrict__ x,
+                     double *__restrict__ y, double *__restrict__ carry_head,
+                     double *__restrict__ carry_tail, long long nchunks, int G, int m) {
+    using VT = float;
+    constexpr int NBT = SIGMA / 4;  // blocks per tile
+    // the carry fixup that follows may launch now; it waits for this grid to finish
+    asm volatile("griddepcontrol.launch_dependents;");
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+    const long long nwarps = (long long)gridDim.x * SPMV_WARPS;
+    constexpr int KSTK = 4;
+    constexpr unsigned SLOT = SPMV_WARPS * 32 * 8;  // bytes between a thread's slots
+    __shared__ __align__(16) double s_piece[KSTK * SPMV_WARPS * 32];
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(&s_piece[threadIdx.x]);
+
+    for (long long c = (long long)blockIdx.x * SPMV_WARPS + w; c < nchunks; c += nwarps) {
+        const ChunkHdr H = hdr[c];
+        const int r_first = H.r_first, r_last = H.r_first + H.nrows - 1;
+        const unsigned shared = H.shared;
+        int carry_row = (shared & 1u) ? r_first : -1;
+        double carry_val = 0.0;
+        const long long t0 = c * G;
+        const VT *vb = vals + t0 * 32 * SIGMA;
+        const IT *cb = cols + t0 * 32 * SIGMA;
+        const VT *xb = x + (sizeof(IT) == 2 ? r_first : 0);  // base of the column offsets
+        const int NB = G * NBT;
+
+        CBlk<IT> c1 = CBlk<IT>::load(cb, 1, lane, pf);
+        CBlk<IT> c2 = CBlk<IT>::load(cb, NB > 2 ? 2 : 1, lane, pf);
+        VBlk<VT> v0 = VBlk<VT>::load(vb, 0, lane, pf), v1 = VBlk<VT>::load(vb, 1, lane, pf);
+        VT x0[4];
+        {
+            const CBlk<IT> c0 = CBlk<IT>::load(cb, 0, lane, pf);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x0[q] = c0.gather(q, xb, pl);
+        }
+        unsigned Fn = ld_stream(desc + t0 * 32 + lane, pf);
+        int rsn = tile_ptr[t0];
+
+#pragma unroll 1
+        for (int tt = 0; tt < G; ++tt) {
+            // tile start: the lanes' row-start masks give each lane its first row
+            const unsigned F = Fn;
+            const int rs = rsn;
+            if (tt + 1 < G) {
+                Fn = ld_stream(desc + (t0 + tt + 1) * 32 + lane, pf);
+                rsn = tile_ptr[t0 + tt + 1];
+            }
+            const int b00 = (int)(__shfl_sync(FULL, F, 0) & 1u);
+            const int nst = __popc(F);
+            const int excl = warp_excl_scan(nst, lane);
+            const int total = __shfl_sync(FULL, excl + nst, 31);
+            const int row0 = rs + excl - b00;  // row open when the lane starts
+            const int rem = G - 1 - tt;        // tiles after this one
+            int rowcur = row0;
+            Acc<VT> acc;
+            double hpiece = 0.0;
+            bool seen = false;
+
+            // The tile's blocks.  Block qb prefetches block qb + d of the chunk (columns d = 3,
+            // values 2, x 1); that block lies (qb + d) / NBT tiles ahead, so only prefetches
+            // past this tile compare against the tiles left.
+            auto walk = [&](auto fast_tag) {
+                constexpr bool FAST = decltype(fast_tag)::value;
+                unsigned sp = sbase;
+#pragma unroll
+                for (int qb = 0; qb < NBT; ++qb) {
+                    CBlk<IT> cn = c2;
+                    VBlk<VT> vn = v1;
+                    if ((qb + 3) / NBT == 0 || rem >= (qb + 3) / NBT)
+                        cn = CBlk<IT>::load(cb, tt * NBT + qb + 3, lane, pf);
+                    if ((qb + 2) / NBT == 0 || rem >= (qb + 2) / NBT)
+                        vn = VBlk<VT>::load(vb, tt * NBT + qb + 2, lane, pf);
+                    VT x1[4];
+                    if ((qb + 1) / NBT == 0 || rem >= (qb + 1) / NBT) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) x1[q] = c1.gather(q, xb, pl);
+                    }
+                    if (FAST) {  // row ends park the piece in the lane's shared slots
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const bool st = (F >> (qb * 4 + q)) & 1u;
+                            acc.push(sp, st);
+                            sp += st ? SLOT : 0u;
+                            acc.add_restart(v0.get(q), x0[q], st);
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            if ((F >> (qb * 4 + q)) & 1u) {
+                                if (seen) {
+                                    if (rowcur < m) y[rowcur] = acc.value();
+                                } else {
+                                    hpiece = acc.value();
+                                    seen = true;
+                                }
+                                ++rowcur;
+                                acc.reset();
+                            }
+                            acc.add(v0.get(q), x0[q]);
+                        }
+                    }
+                    c1 = c2; c2 = cn;
+                    v0 = v1; v1 = vn;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) x0[q] = x1[q];
+                }
+            };
+            if (!__any_sync(FULL, nst > KSTK)) {
+                walk(Flag<true>{});
+                seen = nst > 0;
+                if (seen) hpiece = Acc<VT>::piece_at(sbase);
+                for (int k2 = 1; k2 < nst; ++k2)
+                    if (row0 + k2 < m) y[row0 + k2] = Acc<VT>::piece_at(sbase + k2 * SLOT);
+                rowcur = row0 + nst;
+            } else {
+                walk(Flag<false>{});
+            }
+            const double a = acc.value();
+            tile_combine(seen ? hpiece : a, seen ? a : 0.0, seen, rowcur, rs + total - b00,
+                         lane, r_first, r_last, shared, c, y, carry_head, carry_tail, m,
+                         carry_row, carry_val);
+        }
+        if (carry_row >= 0 && lane == 0)
+            flush_row(carry_row, carry_val, r_first, r_last, shared, c, y, carry_head,
+                      carry_tail, m);
+    }
+}
+
 template <typename VT, typename IT>
 cudaError_t convert_t(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,
                       cudaStream_t s) {
@@ -286,9 +457,16 @@ cudaError_t convert_t(Handle &h, const int *rp, const int *ci, const double *v, 
 
 template <int SG, typename VT, typename IT>
 void launch_sg(const Handle &h, unsigned grid, const void *x, void *y, cudaStream_t s) {
-    csr5_spmv_kernel<SG, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
-        (const ChunkHdr *)h.meta, h.tile_ptr, h.flags, (const VT *)h.vals, (const IT *)h.cols,
-        (const VT *)x, (double *)y, h.carry_head, h.carry_tail, h.nchunks, h.G, h.m);
+    if constexpr (sizeof(VT) == 4)
+        csr5_spmv_f32_kernel<SG, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
+            (const ChunkHdr *)h.meta, h.tile_ptr, h.flags, (const float *)h.vals,
+            (const IT *)h.cols, (const float *)x, (double *)y, h.carry_head, h.carry_tail,
+            h.nchunks, h.G, h.m);
+    else
+        csr5_spmv_kernel<SG, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
+            (const ChunkHdr *)h.meta, h.tile_ptr, h.flags, (const VT *)h.vals,
+            (const IT *)h.cols, (const VT *)x, (double *)y, h.carry_head, h.carry_tail,
+            h.nchunks, h.G, h.m);
 }
 
 template <typename VT, typename IT>
