@@ -88,8 +88,10 @@ csr5_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
     desc[t * 32 + lane] = F;
 }
 
-__global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long nchunks,
-                                 long long L, ChunkHdr *__restrict__ hdr) {
+// Chunk headers.  aux bit 0: the chunk holds elements that read no x (the zero element of an
+// empty row, or the padding of the last chunk); chunks without them skip that check.
+__global__ void chunk_hdr_kernel(const int *__restrict__ arp, const int *__restrict__ rp, int m,
+                                 long long nchunks, long long L, ChunkHdr *__restrict__ hdr) {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nchunks) return;
     const long long s = c * L, e = s + L;
@@ -101,7 +103,10 @@ __global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long n
     hdr[c].r_first = r_first;
     hdr[c].nrows = r_last - r_first + 1;
     hdr[c].shared = sh;
-    hdr[c].aux = 0;
+    unsigned none = r_last >= m ? 1u : 0u;
+    for (int r = r_first; r <= r_last && r < m && !none; ++r)
+        if (rp[r + 1] == rp[r]) none = 1u;
+    hdr[c].aux = (int)none;
 }
 
 // Tile end: the cross-lane combine of the lanes' open row pieces.  head is the piece a lane
@@ -331,6 +336,10 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
         const ChunkHdr H = hdr[c];
         const int r_first = H.r_first, r_last = H.r_first + H.nrows - 1;
         const unsigned shared = H.shared;
+        // chunks without elements that read no x skip the gather's test (16-bit offsets and
+        // tiles of 24 or 32 steps; the other forms gained nothing from it or spilled)
+        constexpr bool SKIP = sizeof(IT) == 2 && SIGMA >= 24;
+        const bool chk = !SKIP || (H.aux & 1);
         int carry_row = (shared & 1u) ? r_first : -1;
         double carry_val = 0.0;
         const long long t0 = c * G;
@@ -373,9 +382,11 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
 
             // The tile's blocks.  Block qb prefetches block qb + d of the chunk (columns d = 3,
             // values 2, x 1); that block lies (qb + d) / NBT tiles ahead, so only prefetches
-            // past this tile compare against the tiles left.
-            auto walk = [&](auto fast_tag) {
+            // past this tile compare against the tiles left.  CHK: the chunk has elements that
+            // read no x, so each gather tests its column.
+            auto walk = [&](auto fast_tag, auto chk_tag) {
                 constexpr bool FAST = decltype(fast_tag)::value;
+                constexpr bool CHK = decltype(chk_tag)::value;
                 unsigned sp = sbase;
 #pragma unroll
                 for (int qb = 0; qb < NBT; ++qb) {
@@ -388,7 +399,8 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
                     VT x1[4];
                     if ((qb + 1) / NBT == 0 || rem >= (qb + 1) / NBT) {
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) x1[q] = c1.gather(q, xb, pl);
+                        for (int q = 0; q < 4; ++q)
+                            x1[q] = CHK ? c1.gather(q, xb, pl) : c1.gather_all(q, xb, pl);
                     }
                     if (FAST) {  // row ends park the piece in the lane's shared slots
 #pragma unroll
@@ -421,14 +433,15 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
                 }
             };
             if (!__any_sync(FULL, nst > KSTK)) {
-                walk(Flag<true>{});
+                if (!SKIP || chk) walk(Flag<true>{}, Flag<true>{});
+                else walk(Flag<true>{}, Flag<false>{});
                 seen = nst > 0;
                 if (seen) hpiece = Acc<VT>::piece_at(sbase);
                 for (int k2 = 1; k2 < nst; ++k2)
                     if (row0 + k2 < m) y[row0 + k2] = Acc<VT>::piece_at(sbase + k2 * SLOT);
                 rowcur = row0 + nst;
             } else {
-                walk(Flag<false>{});
+                walk(Flag<false>{}, Flag<true>{});
             }
             const double a = acc.value();
             tile_combine(seen ? hpiece : a, seen ? a : 0.0, seen, rowcur, rs + total - b00,
@@ -451,7 +464,7 @@ cudaError_t convert_t(Handle &h, const int *rp, const int *ci, const double *v, 
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     chunk_hdr_kernel<<<(unsigned)((h.nchunks + 255) / 256), 256, 0, s>>>(
-        h.arp, h.m, h.nchunks, h.L, (ChunkHdr *)h.meta);
+        h.arp, rp, h.m, h.nchunks, h.L, (ChunkHdr *)h.meta);
     return cudaGetLastError();
 }
 

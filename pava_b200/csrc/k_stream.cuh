@@ -55,6 +55,11 @@ template <> struct CBlk<int> {
         const int c = col(q, 0);
         return c >= 0 ? ld_x(xb + c, pol) : T(0);
     }
+    // the same where every element of the chunk reads x
+    template <typename T>
+    __device__ __forceinline__ T gather_all(int q, const T *xb, uint64_t pol) const {
+        return ld_x(xb + col(q, 0), pol);
+    }
     int4 a;
     __device__ __forceinline__ int col(int q, int) const {
         return q == 0 ? a.x : q == 1 ? a.y : q == 2 ? a.z : a.w;
@@ -72,6 +77,12 @@ template <> struct CBlk<short> {
         const unsigned w = q < 2 ? a.x : a.y;
         const int d = (q & 1) ? ((int)w >> 16) : ((int)(w << 16) >> 16);
         return d != DELTA_NONE ? ld_x(xb + d, pol) : T(0);
+    }
+    template <typename T>
+    __device__ __forceinline__ T gather_all(int q, const T *xb, uint64_t pol) const {
+        const unsigned w = q < 2 ? a.x : a.y;
+        const int d = (q & 1) ? ((int)w >> 16) : ((int)(w << 16) >> 16);
+        return ld_x(xb + d, pol);
     }
     uint2 a;
     __device__ __forceinline__ int col(int q, int r_first) const {

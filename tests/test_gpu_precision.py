@@ -55,6 +55,28 @@ def test_fp32c_irregular(cuda, fmt, kw):
 
 
 @pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
+@pytest.mark.parametrize("index_mode", [_abi.INDEX_I32, _abi.INDEX_DELTA16], ids=["i32", "d16"])
+def test_fp32c_empty_rows_between_full_chunks(cuda, fmt, kw, index_mode):
+    # chunks with and without empty rows side by side (empty rows in two bands only); x is
+    # non-finite where no element reads it: every empty row is exactly 0, every row finite
+    A = M.stencil27(40, seed=11)
+    lens = np.diff(A.rp)
+    keep = np.ones(A.m, bool)
+    keep[20_000:20_050] = False
+    keep[41_000:41_003] = False
+    keep[:5] = False
+    rp = np.concatenate([[0], np.cumsum(np.where(keep, lens, 0))]).astype(np.int32)
+    sel = np.repeat(keep, lens)
+    B = M.from_arrays(A.m, A.n + 2, rp, A.ci[sel], A.v[sel].astype(np.float32).astype(np.float64))
+    x = np.concatenate([M.uniform(A.n, seed=12, fp32=True), [np.inf, np.nan]])
+    y, _ = _run(cuda, B, x, fmt, _abi.PREC_FP32C, index_mode, **kw)
+    assert np.all(y[~keep] == 0.0) and np.all(np.isfinite(y))
+    yr, ab = O.csr_ref(B.rp, B.ci, B.v, x)
+    bad, mx, _ = O.rel_error(y, yr, ab, TOL32)
+    assert bad == 0, mx
+
+
+@pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
 def test_fp64_delta16_equals_i32(cuda, fmt, kw):
     A = M.banded(300_000, 64, 24, seed=7)
     x = M.uniform(A.n, seed=8)
