@@ -15,7 +15,8 @@ graph, and a banded matrix with k right-hand sides; forms picked by the autotune
 
 Each line is one JSON object: device time per product (CUDA events, median of --reps after
 warm-up; every input is larger than the 126 MB L2 except where noted), the compulsory
-algorithmic bytes nnz*(s_v + 4) + 4(m+1) + s_x*n*k + 8*m*k, GB/s and the fraction of the
+algorithmic bytes nnz*(s_v + s_i) + 4(m+1) + s_x*n*k + 8*m*k (s_i: 4 for 32-bit columns, 2 for
+16-bit offsets), GB/s and the fraction of the
 measured HBM copy bandwidth.  Parity with the oracle is the job of tests/test_gpu_batch.py;
 here the graph replay is checked bit for bit against a direct launch, and the multi-RHS
 product's first column against a single-vector product of the same form.
@@ -110,11 +111,13 @@ def run_batch(torch, count, reps, peak, precision):
     yh = y.cpu().numpy()
     assert np.array_equal(yh, b.spmv(x).cpu().numpy()), "graph replay differs from a launch"
     sv = 4 if fp32 else 8
-    alg = b.nnz * (sv + 4) + 4 * (b.m + count) + sv * b.n + 8 * b.m
+    si = 2 if b.info()["index_mode"] == _abi.INDEX_DELTA16 else 4  # column bytes as stored
+    alg = b.nnz * (sv + si) + 4 * (b.m + count) + sv * b.n + 8 * b.m
     gbs = alg / (ms * 1e-3) / 1e9
     return {"workload": "batch", "matrices": count, "rows": b.m, "nnz": b.nnz,
             "precision": "fp32c" if fp32 else "fp64", "form": fmt,
-            "opts": {k: v for k, v in opts.items() if v}, "launch": "cuda graph replay",
+            "opts": {k: v for k, v in opts.items() if v}, "index_bytes": si,
+            "launch": "cuda graph replay",
             "ms": ms, "alg_bytes": alg, "GBps": gbs, "frac_hbm": gbs / peak[0],
             "peak": peak[1], "gen_s": gen_s,
             "create_s": create_s, "autotune": table}
@@ -137,11 +140,13 @@ def run_banded(torch, rows, ks, reps, peak):
             ms, _ = time_it(torch, lambda: mat.spmv(Xd.reshape(-1), Y.reshape(-1)), reps)
         y0 = SpMatrix(A, "csr", lanes_per_row=8).spmv(Xd[:, 0].contiguous()).cpu().numpy()
         mx = float(np.max(np.abs(Y[:, 0].cpu().numpy() - y0)))
-        alg = A.nnz * 12 + 4 * (A.m + 1) + 8 * A.n * k + 8 * A.m * k
+        si = 2 if mat.info()["index_mode"] == _abi.INDEX_DELTA16 else 4  # as stored
+        alg = A.nnz * (8 + si) + 4 * (A.m + 1) + 8 * A.n * k + 8 * A.m * k
         gbs = alg / (ms * 1e-3) / 1e9
         ranked = sorted((x for x in ents if x["ms"] > 0), key=lambda x: x["ms"])
         out.append({"workload": "banded", "rows": A.m, "nnz": A.nnz, "k": k, "precision": "fp64",
-                    "form": e["format"], "opts": opts, "ms": ms, "alg_bytes": alg, "GBps": gbs,
+                    "form": e["format"], "opts": opts, "index_bytes": si, "ms": ms,
+                    "alg_bytes": alg, "GBps": gbs,
                     "frac_hbm": gbs / peak[0], "peak": peak[1], "max_abs_diff_vs_spmv_col0": mx,
                     "candidates": len(ents),
                     "runner_up_ms": ranked[1]["ms"] if len(ranked) > 1 else None,

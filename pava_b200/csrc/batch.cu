@@ -170,7 +170,7 @@ pava_status build_union(int count, const pava_csr *mats, cudaStream_t s, pava_ba
     return PAVA_SUCCESS;
 }
 
-// Built-in candidate forms for k right-hand sides (at most 72 for any k <= 128).
+// Built-in candidate forms for k right-hand sides (at most 72 for any k <= 128; 26 for k = 1).
 std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
     std::vector<std::pair<int, pava_opts>> c;
     auto base = [&]() {
@@ -179,16 +179,20 @@ std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
         o.precision = precision;
         return o;
     };
-    if (k == 1) {
-        for (int S : {64, 128}) {
-            pava_opts o = base();
-            o.steps = S;
-            c.push_back({PAVA_FORMAT_CVR, o});
-        }
-        for (int sg : {16, 32}) {
-            pava_opts o = base();
-            o.sigma = sg;
-            c.push_back({PAVA_FORMAT_CSR5, o});
+    if (k == 1) {  // each with 32-bit columns and with 16-bit offsets where they reach
+        for (int im : {(int)PAVA_INDEX_I32, (int)PAVA_INDEX_AUTO}) {
+            for (int S : {64, 128}) {
+                pava_opts o = base();
+                o.steps = S;
+                o.index_mode = im;
+                c.push_back({PAVA_FORMAT_CVR, o});
+            }
+            for (int sg : {16, 32}) {
+                pava_opts o = base();
+                o.sigma = sg;
+                o.index_mode = im;
+                c.push_back({PAVA_FORMAT_CSR5, o});
+            }
         }
     }
     const int kpls[3] = {1, 2, 4};

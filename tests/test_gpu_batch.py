@@ -236,6 +236,9 @@ def test_autotune_k1_runs_every_candidate(cuda):
     ents, best = autotune(A, k=1, reps=3)
     forms = {e["format"] for e in ents}
     assert {"cvr", "csr5", "csr"} <= forms
+    # CVR / CSR5 come with 32-bit columns and with 16-bit offsets where they reach
+    modes = {(e["format"], e["opts"]["index_mode"]) for e in ents if e["format"] != "csr"}
+    assert modes == {(f, m) for f in ("cvr", "csr5") for m in (_abi.INDEX_I32, _abi.INDEX_AUTO)}
     assert all(e["ms"] > 0 and e["status"] == 0 for e in ents)
     assert ents[best]["ms"] == min(e["ms"] for e in ents)
     # the winner computes the right product
