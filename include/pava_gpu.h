@@ -209,7 +209,8 @@ pava_status pava_batch_destroy(pava_batch *b);
  * Converts A into every built-in candidate form for k right-hand sides and times each (two
  * warm-up calls, then the median of `reps` CUDA-event timings of the SpMV/SpMM with x and y
  * already on the device).  Candidates: for k = 1, CVR steps 64/128 and CSR5 sigma 16/32, each
- * with 32-bit columns and with PAVA_INDEX_AUTO (16-bit offsets where they reach); for
+ * with 32-bit columns and with PAVA_INDEX_AUTO (16-bit offsets where they reach), CSR5 also
+ * with the tiles per chunk that fill the last wave of warp chunks best (1..8); for
  * every k, the CSR row-group form over lanes_per_row x col_lanes x cols_per_lane x
  * rows_per_tile, and for k > 1 also with x_window.  entries[0 .. *n_entries) receive every candidate (ms < 0 when it failed,
  * with its status), *best the index of the fastest.  No counterpart in the reference. */

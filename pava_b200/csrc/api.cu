@@ -349,8 +349,7 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
         if (o.tiles_per_chunk) {
             h.G = o.tiles_per_chunk;
         } else {  // 4 tiles per chunk, fewer for small matrices
-            const long long tiles = (long long)h.nnz / (32LL * h.sigma);
-            h.G = tiles >= 4 * want_chunks ? 4 : (tiles >= 2 * want_chunks ? 2 : 1);
+            h.G = pava::csr5_default_tiles((long long)h.nnz / (32LL * h.sigma), want_chunks);
         }
         if (!(h.sigma == 8 || h.sigma == 12 || h.sigma == 16 || h.sigma == 24 || h.sigma == 32) ||
             h.G < 1 || h.G > 64) {

@@ -170,8 +170,10 @@ pava_status build_union(int count, const pava_csr *mats, cudaStream_t s, pava_ba
     return PAVA_SUCCESS;
 }
 
-// Built-in candidate forms for k right-hand sides (at most 72 for any k <= 128; 26 for k = 1).
-std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
+// Built-in candidate forms for k right-hand sides (at most 72 for any k <= 128; 30 for k = 1).
+// nnz and sm_count size the CSR5 chunks.
+std::vector<std::pair<int, pava_opts>> candidates(int k, int precision, long long nnz,
+                                                  int sm_count) {
     std::vector<std::pair<int, pava_opts>> c;
     auto base = [&]() {
         pava_opts o;
@@ -187,11 +189,17 @@ std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
                 o.index_mode = im;
                 c.push_back({PAVA_FORMAT_CVR, o});
             }
-            for (int sg : {16, 32}) {
+            for (int sg : {16, 32}) {  // default tiles per chunk, and wave-balanced
                 pava_opts o = base();
                 o.sigma = sg;
                 o.index_mode = im;
                 c.push_back({PAVA_FORMAT_CSR5, o});
+                const long long tiles = nnz / (32LL * sg), warps = 24LL * sm_count;
+                const int gw = pava::csr5_wave_tiles(tiles, warps);
+                if (gw != pava::csr5_default_tiles(tiles, warps)) {
+                    o.tiles_per_chunk = gw;
+                    c.push_back({PAVA_FORMAT_CSR5, o});
+                }
             }
         }
     }
@@ -238,7 +246,11 @@ pava_status pava_autotune(const pava_csr *A, int k, int precision, int reps,
     if (reps < 1) reps = 1;
     *n_entries = 0;
     *best = -1;
-    const std::vector<std::pair<int, pava_opts>> cand = candidates(k, precision);
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return bfail(PAVA_E_CUDA, "no usable CUDA device");
+    const std::vector<std::pair<int, pava_opts>> cand = candidates(k, precision, A->nnz, sms);
     const size_t sx = precision == PAVA_PREC_FP32C ? 4 : 8;
     void *X = nullptr, *Y = nullptr;
     cudaError_t e = cudaMalloc(&X, sx * (size_t)(A->n ? A->n : 1) * k);

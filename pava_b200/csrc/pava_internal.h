@@ -66,6 +66,25 @@ struct Handle {
 // Sets the message pava_last_error() returns on this thread.
 void set_last_error(const std::string &msg);
 
+// CSR5 tiles per chunk.  The persistent grid keeps `warps` warps resident (24 per SM); each
+// takes chunks in turn, so a chunk count just above a multiple of `warps` leaves a last wave
+// that few warps run.
+// Default: 4 tiles per chunk, fewer when that leaves fewer chunks than warps.
+inline int csr5_default_tiles(long long tiles, long long warps) {
+    return tiles >= 4 * warps ? 4 : (tiles >= 2 * warps ? 2 : 1);
+}
+// Wave-balanced: the G in 1..8 with the fewest tiles on a warp's critical path,
+// ceil(tiles / (G * warps)) * G; the largest G among equals.
+inline int csr5_wave_tiles(long long tiles, long long warps) {
+    int best = 1;
+    long long best_t = -1;
+    for (int g = 1; g <= 8; ++g) {
+        const long long t = (tiles + g * warps - 1) / (g * warps) * g;
+        if (best_t < 0 || t <= best_t) { best_t = t; best = g; }
+    }
+    return best;
+}
+
 // Kernel launchers (stream-ordered; return cudaGetLastError()).
 cudaError_t launch_validate(const int *rp, const int *ci, int m, int n, int nnz, int *d_err,
                             cudaStream_t s);
