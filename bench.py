@@ -12,7 +12,9 @@ steps as it does in any SpMV loop.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pava|reference]
 
 Under torchrun (N > 1) every rank runs its own replica (the path has no exchange step);
-time is the max over ranks and value the aggregate of all ranks.
+time is the max over ranks and value the aggregate of all ranks.  At N = 1 the line also
+carries `precision_form`: FP64 against the FP32-compensated form on the 128^3 27-point
+stencil (speed-up and error), measured after the timed region (--no-precision skips it).
 """
 from __future__ import annotations
 
@@ -44,6 +46,8 @@ def parse():
     p.add_argument("--impl", choices=["pava", "reference"], default="pava")
     p.add_argument("--rows", type=int, default=4_194_304, help="smaller sizes for smoke runs")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-precision", action="store_true",
+                   help="skip the FP64 vs FP32C comparison on the 27-point stencil")
     p.add_argument("--variants", default="cvr:steps=64,cvr:steps=128,csr5:sigma=16,csr5:sigma=32",
                    help="FP64 candidates for the chosen variant")
     return p.parse_args()
@@ -391,10 +395,68 @@ def main():
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.no_precision:
+            line["precision_form"] = precision_form(torch, stream)
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def precision_form(torch, stream):
+    """The precision form on the 128^3 27-point stencil (2,097,152 rows, 55.7 M nnz, values and
+    x FP32-representable): the fastest FP64 form against the fastest FP32C form (FP32 values
+    and x, 16-bit column offsets, compensated FP32 accumulation, FP64 carries) of the same
+    small sweep (CSR5 sigma 32 with 4 and 8 tiles per chunk; CVR steps 128), each timed as
+    whole SpMVs (kernel + carry fixup) back to back, 30 after 5 warm-ups; the FP32C result's
+    relative error per row against the FP64 result (cancellation-aware denominator)."""
+    from pava_b200 import _abi
+    from pava_b200 import matrices as M
+    from pava_b200.api import SpMatrix
+    try:
+        A = M.stencil27(128, seed=2)
+        xh = M.uniform(A.n, seed=3, fp32=True)
+        sp = stream.cuda_stream
+        x64 = torch.from_numpy(xh).cuda()
+        x32 = x64.float()
+        sweep = [("csr5", dict(sigma=32)), ("csr5", dict(sigma=32, tiles_per_chunk=8)),
+                 ("cvr", dict(steps=128))]
+        out, ys = {}, {}
+        for prec, x, extra in ((_abi.PREC_FP64, x64, {}),
+                               (_abi.PREC_FP32C, x32, dict(index_mode=_abi.INDEX_DELTA16))):
+            best = None
+            for fmt, kw in sweep:
+                mat = SpMatrix(A, fmt, precision=prec, **kw, **extra)
+                y = torch.empty(A.m, dtype=torch.float64, device="cuda")
+                with torch.cuda.stream(stream):
+                    for _ in range(5):
+                        mat.spmv_raw(x.data_ptr(), y.data_ptr(), sp, 0)
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    for _ in range(30):
+                        mat.spmv_raw(x.data_ptr(), y.data_ptr(), sp, 0)
+                    b.record(stream)
+                b.synchronize()
+                ms = a.elapsed_time(b) / 30
+                name = fmt + "".join(f"_{k}{v}" for k, v in kw.items())
+                if best is None or ms < best[1]:
+                    best = (name, ms)
+                    ys[prec] = y.cpu().numpy()
+                mat.close()
+            key = "fp64" if prec == _abi.PREC_FP64 else "fp32c"
+            out[key] = {"form": best[0], "ms": round(best[1], 6)}
+        rows = np.repeat(np.arange(A.m, dtype=np.int64), np.diff(A.rp))
+        absum = np.bincount(rows, weights=np.abs(A.v) * np.abs(xh[A.ci]), minlength=A.m)
+        y64, y32 = ys[_abi.PREC_FP64], ys[_abi.PREC_FP32C]
+        rel = np.abs(y32 - y64) / np.maximum(np.maximum(np.abs(y64), absum), 1e-300)
+        out.update({"workload": "128^3 27-point stencil, 2,097,152 rows, "
+                                f"{A.nnz:,} nnz, values and x FP32-representable",
+                    "speedup_fp32c_over_fp64": round(out["fp64"]["ms"] / out["fp32c"]["ms"], 3),
+                    "max_rel_err_vs_fp64": float(rel.max()),
+                    "mean_rel_err_vs_fp64": float(rel.mean()), "error_bound": 1e-9})
+        return out
+    except Exception as e:  # a side measurement; the headline line stands without it
+        return {"unavailable": f"failed: {e}"}
 
 
 def cpu_baseline(A, x, alg):
