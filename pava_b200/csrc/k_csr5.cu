@@ -47,7 +47,7 @@ csr5_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                     const double *__restrict__ v, const int *__restrict__ arp, int m,
                     long long ntiles, int sigma, int G, VT *__restrict__ vals,
                     IT *__restrict__ cols, unsigned *__restrict__ desc,
-                    int *__restrict__ tile_ptr, int *ovf) {
+                    int *__restrict__ tile_ptr, ChunkHdr *__restrict__ hdr, int *ovf) {
     const int lane = threadIdx.x & 31;
     const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (t >= ntiles) return;
@@ -68,6 +68,7 @@ csr5_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
     src_of(row);
     int next_start = arp[row + 1];
     unsigned F = 0;
+    bool reads_none = false;  // some element of the lane reads no x
     for (int i = 0; i < sigma; ++i) {
         const long long e = e0 + i;
         while ((long long)next_start <= e) {
@@ -81,17 +82,21 @@ csr5_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
         if (!dummy) {
             val = v[e + rbase];
             col = ci[e + rbase];
+        } else {
+            reads_none = true;
         }
         vals[tbase + vals_offset<VT>(i, lane)] = (VT)val;
         cols[tbase + cols_offset(i, lane)] = enc_col<IT>(col, r_first, ovf);
     }
     desc[t * 32 + lane] = F;
+    if (reads_none) atomicOr(&hdr[t / G].aux, 1);
 }
 
-// Chunk headers.  aux bit 0: the chunk holds elements that read no x (the zero element of an
-// empty row, or the padding of the last chunk); chunks without them skip that check.
-__global__ void chunk_hdr_kernel(const int *__restrict__ arp, const int *__restrict__ rp, int m,
-                                 long long nchunks, long long L, ChunkHdr *__restrict__ hdr) {
+// Chunk headers.  aux bit 0 (set by csr5_convert_kernel, which runs after this kernel): the
+// chunk holds elements that read no x (the zero element of an empty row, or the padding of
+// the last chunk); chunks without them skip that check.
+__global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long nchunks,
+                                 long long L, ChunkHdr *__restrict__ hdr) {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nchunks) return;
     const long long s = c * L, e = s + L;
@@ -103,10 +108,7 @@ __global__ void chunk_hdr_kernel(const int *__restrict__ arp, const int *__restr
     hdr[c].r_first = r_first;
     hdr[c].nrows = r_last - r_first + 1;
     hdr[c].shared = sh;
-    unsigned none = r_last >= m ? 1u : 0u;
-    for (int r = r_first; r <= r_last && r < m && !none; ++r)
-        if (rp[r + 1] == rp[r]) none = 1u;
-    hdr[c].aux = (int)none;
+    hdr[c].aux = 0;
 }
 
 // Tile end: the cross-lane combine of the lanes' open row pieces.  head is the piece a lane
@@ -457,14 +459,14 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
 template <typename VT, typename IT>
 cudaError_t convert_t(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,
                       cudaStream_t s) {
+    chunk_hdr_kernel<<<(unsigned)((h.nchunks + 255) / 256), 256, 0, s>>>(
+        h.arp, h.m, h.nchunks, h.L, (ChunkHdr *)h.meta);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
     const long long blocks = (h.ntiles * 32 + 255) / 256;
     csr5_convert_kernel<VT, IT><<<(unsigned)blocks, 256, 0, s>>>(
         rp, ci, v, h.arp, h.m, h.ntiles, h.sigma, h.G, (VT *)h.vals, (IT *)h.cols, h.flags,
-        h.tile_ptr, ovf);
-    cudaError_t err = cudaGetLastError();
-    if (err != cudaSuccess) return err;
-    chunk_hdr_kernel<<<(unsigned)((h.nchunks + 255) / 256), 256, 0, s>>>(
-        h.arp, rp, h.m, h.nchunks, h.L, (ChunkHdr *)h.meta);
+        h.tile_ptr, (ChunkHdr *)h.meta, ovf);
     return cudaGetLastError();
 }
 
