@@ -115,7 +115,9 @@ __global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long n
 // adds to the row open at its start (its whole sum when no row starts in the lane), tail the
 // sum since the lane's last row start (seen: a row starts in the lane), rowcur the row of that
 // tail, next_row the row open at the tile's end.  Rows that end in the tile go to y (or to
-// the chunk's carry slots); the open row's sum stays in carry_row / carry_val.
+// the chunk's carry slots); the open row's sum stays in carry_row / carry_val.  The FP64
+// kernel has the same steps inline: calling this helper there changed its register allocation
+// and doubled its spills at 80 registers.
 __device__ __forceinline__ void tile_combine(double head, double tail, bool seen, int rowcur,
                                              int next_row, int lane, int r_first, int r_last,
                                              unsigned shared, long long c, double *y,
