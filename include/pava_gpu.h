@@ -53,8 +53,9 @@ typedef enum pava_precision {
 
 typedef enum pava_index_mode {
     PAVA_INDEX_I32 = 0,     /* 32-bit column indices */
-    PAVA_INDEX_DELTA16 = 1, /* 16-bit column offsets from the chunk's first row (every offset
-                               within +-32767, else PAVA_E_UNSUPPORTED_PARAMS) */
+    PAVA_INDEX_DELTA16 = 1, /* 16-bit column offsets from a per-chunk base column, the middle
+                               of the chunk's column range (every chunk's columns within a
+                               span of 65534, else PAVA_E_UNSUPPORTED_PARAMS) */
     PAVA_INDEX_AUTO = 2     /* CVR / CSR5: 16-bit offsets when every column fits, otherwise
                                32-bit columns (pava_info.index_mode tells which); same results */
 } pava_index_mode;

@@ -99,13 +99,14 @@ void free_handle_buffers(pava::Handle &h) {
     cudaFree(h.flags);
     cudaFree(h.meta);
     cudaFree(h.tile_ptr);
+    cudaFree(h.colbase);
     cudaFree(h.carry_head);
     cudaFree(h.carry_tail);
     cudaFree(h.rp);
     cudaFree(h.ci);
     cudaFree(h.v);
     h.arp = nullptr; h.vals = nullptr; h.cols = nullptr; h.flags = nullptr; h.meta = nullptr;
-    h.tile_ptr = nullptr; h.carry_head = nullptr; h.carry_tail = nullptr;
+    h.tile_ptr = nullptr; h.colbase = nullptr; h.carry_head = nullptr; h.carry_tail = nullptr;
     h.rp = nullptr; h.ci = nullptr; h.v = nullptr;
 }
 
@@ -207,6 +208,10 @@ pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double 
         h.device_bytes += si * padded;
         PAVA_CUDA(dalloc(&h.carry_head, (size_t)h.nchunks, &h.device_bytes), "cudaMalloc(carry)");
         PAVA_CUDA(dalloc(&h.carry_tail, (size_t)h.nchunks, &h.device_bytes), "cudaMalloc(carry)");
+        if (h.index_mode == PAVA_INDEX_DELTA16) {
+            PAVA_CUDA(dalloc(&h.colbase, (size_t)h.nchunks, &h.device_bytes), "cudaMalloc(colbase)");
+            PAVA_CUDA(pava::chunk_colbase(h, rp, ci, s), "chunk column bases");
+        }
         int *d_ovf = nullptr;
         PAVA_CUDA(cudaMallocAsync(&d_ovf, sizeof(int), s), "cudaMallocAsync");
         cudaError_t e = cudaMemsetAsync(d_ovf, 0, sizeof(int), s);
@@ -233,7 +238,7 @@ pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double 
         h.d16_overflow = ovf ? 1 : 0;
         if (ovf)
             return fail(PAVA_E_UNSUPPORTED_PARAMS,
-                        "16-bit column offsets: a column lies more than 32767 from its chunk's first row");
+                        "16-bit column offsets: a chunk's columns span more than 65534");
     } else {  // plain CSR: private copies (values narrowed to float for FP32C)
         PAVA_CUDA(dalloc(&h.rp, (size_t)h.m + 1, &h.device_bytes), "cudaMalloc(rp)");
         PAVA_CUDA(dalloc(&h.ci, (size_t)h.nnz, &h.device_bytes), "cudaMalloc(ci)");

@@ -32,11 +32,11 @@ namespace pava {
 
 namespace {
 
-template <typename IT> __device__ __forceinline__ IT enc_col(int col, int r_first, int *ovf);
+template <typename IT> __device__ __forceinline__ IT enc_col(int col, int base, int *ovf);
 template <> __device__ __forceinline__ int enc_col<int>(int col, int, int *) { return col; }
-template <> __device__ __forceinline__ short enc_col<short>(int col, int r_first, int *ovf) {
+template <> __device__ __forceinline__ short enc_col<short>(int col, int base, int *ovf) {
     if (col < 0) return DELTA_NONE;
-    const int d = col - r_first;
+    const int d = col - base;
     if (d < -32767 || d > 32767) { atomicOr(ovf, 1); return DELTA_NONE; }
     return (short)d;
 }
@@ -47,13 +47,14 @@ csr5_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                     const double *__restrict__ v, const int *__restrict__ arp, int m,
                     long long ntiles, int sigma, int G, VT *__restrict__ vals,
                     IT *__restrict__ cols, unsigned *__restrict__ desc,
-                    int *__restrict__ tile_ptr, ChunkHdr *__restrict__ hdr, int *ovf) {
+                    int *__restrict__ tile_ptr, ChunkHdr *__restrict__ hdr,
+                    const int *__restrict__ colbase, int *ovf) {
     const int lane = threadIdx.x & 31;
     const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (t >= ntiles) return;
     const int nr = m + 2;
     const long long tbase = t * 32LL * sigma;
-    const int r_first = upper_bound_m1(arp, nr, (t / G) * 32LL * sigma * G);  // chunk's first row
+    const int col_base = sizeof(IT) == 2 ? colbase[t / G] : 0;  // of the 16-bit offsets
     const long long e0 = tbase + (long long)lane * sigma;
     int row = upper_bound_m1(arp, nr, e0);
     if (lane == 0) tile_ptr[t] = row;
@@ -86,17 +87,19 @@ csr5_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             reads_none = true;
         }
         vals[tbase + vals_offset<VT>(i, lane)] = (VT)val;
-        cols[tbase + cols_offset(i, lane)] = enc_col<IT>(col, r_first, ovf);
+        cols[tbase + cols_offset(i, lane)] = enc_col<IT>(col, col_base, ovf);
     }
     desc[t * 32 + lane] = F;
     if (reads_none) atomicOr(&hdr[t / G].aux, 1);
 }
 
-// Chunk headers.  aux bit 0 (set by csr5_convert_kernel, which runs after this kernel): the
-// chunk holds elements that read no x (the zero element of an empty row, or the padding of
-// the last chunk); chunks without them skip that check.
-__global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long nchunks,
-                                 long long L, ChunkHdr *__restrict__ hdr) {
+// Chunk headers.  aux bits 1..31: the base column of the chunk's 16-bit offsets (colbase,
+// when the form has them), read with the header; bit 0 (set by csr5_convert_kernel, which
+// runs after this kernel): the chunk holds elements that read no x (the zero element of an
+// empty row, or the padding of the last chunk); chunks without them skip that check.
+__global__ void chunk_hdr_kernel(const int *__restrict__ arp, const int *__restrict__ colbase,
+                                 int m, long long nchunks, long long L,
+                                 ChunkHdr *__restrict__ hdr) {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nchunks) return;
     const long long s = c * L, e = s + L;
@@ -108,7 +111,7 @@ __global__ void chunk_hdr_kernel(const int *__restrict__ arp, int m, long long n
     hdr[c].r_first = r_first;
     hdr[c].nrows = r_last - r_first + 1;
     hdr[c].shared = sh;
-    hdr[c].aux = 0;
+    hdr[c].aux = colbase ? (int)((unsigned)colbase[c] << 1) : 0;
 }
 
 // Tile end: the cross-lane combine of the lanes' open row pieces.  head is the piece a lane
@@ -189,7 +192,7 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
         const long long t0 = c * G;
         const VT *vb = vals + t0 * 32 * SIGMA;
         const IT *cb = cols + t0 * 32 * SIGMA;
-        const VT *xb = x + (sizeof(IT) == 2 ? r_first : 0);  // base of the column offsets
+        const VT *xb = x + (sizeof(IT) == 2 ? (int)((unsigned)H.aux >> 1) : 0);  // offsets' base
         const int NB = G * NBT;
 
         CBlk<IT> c1 = CBlk<IT>::load(cb, 1, lane, pf);
@@ -349,7 +352,7 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
         const long long t0 = c * G;
         const VT *vb = vals + t0 * 32 * SIGMA;
         const IT *cb = cols + t0 * 32 * SIGMA;
-        const VT *xb = x + (sizeof(IT) == 2 ? r_first : 0);  // base of the column offsets
+        const VT *xb = x + (sizeof(IT) == 2 ? (int)((unsigned)H.aux >> 1) : 0);  // offsets' base
         const int NB = G * NBT;
 
         CBlk<IT> c1 = CBlk<IT>::load(cb, 1, lane, pf);
@@ -462,13 +465,13 @@ template <typename VT, typename IT>
 cudaError_t convert_t(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,
                       cudaStream_t s) {
     chunk_hdr_kernel<<<(unsigned)((h.nchunks + 255) / 256), 256, 0, s>>>(
-        h.arp, h.m, h.nchunks, h.L, (ChunkHdr *)h.meta);
+        h.arp, h.colbase, h.m, h.nchunks, h.L, (ChunkHdr *)h.meta);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     const long long blocks = (h.ntiles * 32 + 255) / 256;
     csr5_convert_kernel<VT, IT><<<(unsigned)blocks, 256, 0, s>>>(
         rp, ci, v, h.arp, h.m, h.ntiles, h.sigma, h.G, (VT *)h.vals, (IT *)h.cols, h.flags,
-        h.tile_ptr, (ChunkHdr *)h.meta, ovf);
+        h.tile_ptr, (ChunkHdr *)h.meta, h.colbase, ovf);
     return cudaGetLastError();
 }
 
@@ -477,13 +480,13 @@ void launch_sg(const Handle &h, unsigned grid, const void *x, void *y, cudaStrea
     if constexpr (sizeof(VT) == 4)
         csr5_spmv_f32_kernel<SG, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
             (const ChunkHdr *)h.meta, h.tile_ptr, h.flags, (const float *)h.vals,
-            (const IT *)h.cols, (const float *)x, (double *)y, h.carry_head, h.carry_tail,
-            h.nchunks, h.G, h.m);
+            (const IT *)h.cols, (const float *)x, (double *)y, h.carry_head,
+            h.carry_tail, h.nchunks, h.G, h.m);
     else
         csr5_spmv_kernel<SG, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
             (const ChunkHdr *)h.meta, h.tile_ptr, h.flags, (const VT *)h.vals,
-            (const IT *)h.cols, (const VT *)x, (double *)y, h.carry_head, h.carry_tail,
-            h.nchunks, h.G, h.m);
+            (const IT *)h.cols, (const VT *)x, (double *)y, h.carry_head,
+            h.carry_tail, h.nchunks, h.G, h.m);
 }
 
 template <typename VT, typename IT>

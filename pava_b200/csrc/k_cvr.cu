@@ -49,11 +49,11 @@ __device__ __forceinline__ RowSrc row_src(const int *rp, const int *arp, int m, 
     return r;
 }
 
-template <typename IT> __device__ __forceinline__ IT encode_col(int col, int r_first, int *ovf);
+template <typename IT> __device__ __forceinline__ IT encode_col(int col, int base, int *ovf);
 template <> __device__ __forceinline__ int encode_col<int>(int col, int, int *) { return col; }
-template <> __device__ __forceinline__ short encode_col<short>(int col, int r_first, int *ovf) {
+template <> __device__ __forceinline__ short encode_col<short>(int col, int base, int *ovf) {
     if (col < 0) return DELTA_NONE;
-    const int d = col - r_first;
+    const int d = col - base;
     if (d < -32767 || d > 32767) { atomicOr(ovf, 1); return DELTA_NONE; }
     return (short)d;
 }
@@ -61,7 +61,7 @@ template <> __device__ __forceinline__ short encode_col<short>(int col, int r_fi
 template <typename VT, typename IT>
 __device__ __forceinline__ void put_elem(VT *vals, IT *cols, long long cbase, int i, int lane,
                                          const int *ci, const double *v, int e, RowSrc src,
-                                         int r_first, int *ovf) {
+                                         int col_base, int *ovf) {
     double val = 0.0;
     int col = -1;
     if (!src.dummy) {
@@ -69,7 +69,7 @@ __device__ __forceinline__ void put_elem(VT *vals, IT *cols, long long cbase, in
         col = ci[e + src.base];
     }
     vals[cbase + vals_offset<VT>(i, lane)] = (VT)val;
-    cols[cbase + cols_offset(i, lane)] = encode_col<IT>(col, r_first, ovf);
+    cols[cbase + cols_offset(i, lane)] = encode_col<IT>(col, col_base, ovf);
 }
 
 constexpr int CONV_WARPS = 4;
@@ -79,7 +79,8 @@ __global__ void __launch_bounds__(CONV_WARPS * 32)
 cvr_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                    const double *__restrict__ v, const int *__restrict__ arp, int m,
                    long long nchunks, int S, VT *__restrict__ vals, IT *__restrict__ cols,
-                   unsigned *__restrict__ flags, CvrMeta *__restrict__ meta, int *ovf) {
+                   unsigned *__restrict__ flags, CvrMeta *__restrict__ meta,
+                   const int *__restrict__ colbase, int *ovf) {
     __shared__ int s_len[CONV_WARPS][64];
     __shared__ int s_src[CONV_WARPS][64];
     __shared__ int s_row[CONV_WARPS][64];
@@ -93,6 +94,7 @@ cvr_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
     const int r_first = upper_bound_m1(arp, nr, s);
     const int r_last = upper_bound_m1(arp, nr, e - 1);
     const int nrows = r_last - r_first + 1;
+    const int col_base = sizeof(IT) == 2 ? colbase[c] : 0;  // of the 16-bit offsets
     const unsigned lt = lanemask_lt();
 
     int g = lane, row = -1, cur = 0, rem = 0;
@@ -121,7 +123,7 @@ cvr_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             }
             next_g += __popc(b);
         }
-        put_elem<VT, IT>(vals, cols, s, i, lane, ci, v, cur, src, r_first, ovf);
+        put_elem<VT, IT>(vals, cols, s, i, lane, ci, v, cur, src, col_base, ovf);
         ++cur;
         --rem;
         if (rem == 0) fword |= 1u << (i & 31);
@@ -178,7 +180,7 @@ cvr_convert_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
         int slen = s_len[w][j], sa = s_src[w][j];
         src = row_src(rp, arp, m, s_row[w][j]);
         for (int t = 0; t < T; ++t, ++i) {
-            put_elem<VT, IT>(vals, cols, s, i, lane, ci, v, sa + off, src, r_first, ovf);
+            put_elem<VT, IT>(vals, cols, s, i, lane, ci, v, sa + off, src, col_base, ovf);
             ++off;
             const bool slot_end = (off == slen);
             if (slot_end || t == T - 1) fword |= 1u << (i & 31);
@@ -228,9 +230,9 @@ template <int S, typename VT, typename IT>
 __global__ void __launch_bounds__(SPMV_WARPS * 32, sizeof(VT) == 8 ? PAVA_CVR_MINB : PAVA_CVR_MINB32)
 cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ flags,
                 const VT *__restrict__ vals, const IT *__restrict__ cols,
-                const VT *__restrict__ x, double *__restrict__ y,
-                double *__restrict__ carry_head, double *__restrict__ carry_tail,
-                long long nchunks, int m) {
+                const VT *__restrict__ x, const int *__restrict__ colbase,
+                double *__restrict__ y, double *__restrict__ carry_head,
+                double *__restrict__ carry_tail, long long nchunks, int m) {
     constexpr int L = 32 * S;
     constexpr int NB = S / 4;
     __shared__ double s_tail[SPMV_WARPS][64];
@@ -250,7 +252,7 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
         const int i_t = M->i_t;
         const VT *vb = vals + c * L;
         const IT *cb = cols + c * L;
-        const VT *xb = x + (sizeof(IT) == 2 ? r_first : 0);  // base of the column offsets
+        const VT *xb = x + (sizeof(IT) == 2 ? colbase[c] : 0);  // base of the column offsets
         const unsigned *fb = flags + c * S;
         auto LF = [&](int b) { return ld_flag(fb + ((4 * b) >> 5) * 32 + lane); };
 
@@ -361,7 +363,7 @@ cudaError_t convert_t(Handle &h, const int *rp, const int *ci, const double *v, 
     const long long blocks = (h.nchunks + CONV_WARPS - 1) / CONV_WARPS;
     cvr_convert_kernel<VT, IT><<<(unsigned)blocks, CONV_WARPS * 32, 0, s>>>(
         rp, ci, v, h.arp, h.m, h.nchunks, h.S, (VT *)h.vals, (IT *)h.cols, h.flags,
-        (CvrMeta *)h.meta, ovf);
+        (CvrMeta *)h.meta, h.colbase, ovf);
     return cudaGetLastError();
 }
 
@@ -376,18 +378,18 @@ cudaError_t spmv_t(const Handle &h, const void *x, void *y, cudaStream_t s) {
     switch (h.S) {
         case 32:
             cvr_spmv_kernel<32, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
-                meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, yv, h.carry_head,
-                h.carry_tail, h.nchunks, h.m);
+                meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, h.colbase, yv,
+                h.carry_head, h.carry_tail, h.nchunks, h.m);
             break;
         case 64:
             cvr_spmv_kernel<64, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
-                meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, yv, h.carry_head,
-                h.carry_tail, h.nchunks, h.m);
+                meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, h.colbase, yv,
+                h.carry_head, h.carry_tail, h.nchunks, h.m);
             break;
         case 128:
             cvr_spmv_kernel<128, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
-                meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, yv, h.carry_head,
-                h.carry_tail, h.nchunks, h.m);
+                meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, h.colbase, yv,
+                h.carry_head, h.carry_tail, h.nchunks, h.m);
             break;
         default:
             return cudaErrorInvalidValue;

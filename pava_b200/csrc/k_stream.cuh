@@ -10,7 +10,7 @@
 //               float  -- FP32 values and x, compensated accumulation (TwoProduct by FMA,
 //                         TwoSum), the sum and its correction widened to FP64 at the end.
 // Column forms: int    -- 32-bit columns;
-//               short  -- 16-bit offsets from the chunk's first row (col = r_first + d), with
+//               short  -- 16-bit offsets from the chunk's base column (col = base + d), with
 //                         d = -32768 marking an element that reads no x.
 #pragma once
 #include "pava_common.cuh"
@@ -71,7 +71,7 @@ template <> struct CBlk<int> {
     }
 };
 template <> struct CBlk<short> {
-    // x of element q: xb = x + (the chunk's first row); the offset DELTA_NONE reads nothing
+    // x of element q: xb = x + (the chunk's base column); the offset DELTA_NONE reads nothing
     template <typename T>
     __device__ __forceinline__ T gather(int q, const T *xb, uint64_t pol) const {
         const unsigned w = q < 2 ? a.x : a.y;
@@ -85,10 +85,10 @@ template <> struct CBlk<short> {
         return ld_x(xb + d, pol);
     }
     uint2 a;
-    __device__ __forceinline__ int col(int q, int r_first) const {
+    __device__ __forceinline__ int col(int q, int base) const {
         const unsigned w = q < 2 ? a.x : a.y;
         const int d = (q & 1) ? ((int)w >> 16) : ((int)(w << 16) >> 16);
-        return d == DELTA_NONE ? -1 : r_first + d;
+        return d == DELTA_NONE ? -1 : base + d;
     }
     __device__ __forceinline__ static CBlk load(const short *base, int blk, int lane, uint64_t pol) {
         CBlk r;

@@ -73,6 +73,43 @@ __global__ void carry_fixup_kernel(const char *__restrict__ meta, size_t stride,
     }
 }
 
+// Warp per chunk.  Chunk c holds the augmented elements [c*L, (c+1)*L); augmentation only
+// inserts zero elements, so its nonzeros are the CSR's positions [p0, p1).  base = midpoint of
+// their smallest and largest column: 16-bit offsets then reach any chunk whose columns span
+// at most 65,534 (a chunk without nonzeros gets 0).
+__global__ void chunk_colbase_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
+                                     const int *__restrict__ arp, int m, long long nchunks,
+                                     long long L, int *__restrict__ colbase) {
+    const int lane = threadIdx.x & 31;
+    const long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= nchunks) return;  // warp-uniform
+    const long long s = c * L, e = s + L;
+    const int nr = m + 2;
+    // CSR position of augmented element `at`, clamped to row r's nonzeros
+    auto pos = [&](int r, long long at) -> long long {
+        if (r >= m) return rp[m];
+        const long long len = rp[r + 1] - rp[r];
+        long long off = at - arp[r];
+        off = off < 0 ? 0 : (off > len ? len : off);
+        return rp[r] + off;
+    };
+    const long long p0 = pos(upper_bound_m1(arp, nr, s), s);
+    const long long p1 = pos(upper_bound_m1(arp, nr, e - 1), e);
+    int mn = 0x7fffffff, mx = -1;
+    for (long long p = p0 + lane; p < p1; p += 32) {
+        const int col = ci[p];
+        mn = col < mn ? col : mn;
+        mx = col > mx ? col : mx;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const int a = __shfl_xor_sync(FULL, mn, o), b = __shfl_xor_sync(FULL, mx, o);
+        mn = a < mn ? a : mn;
+        mx = b > mx ? b : mx;
+    }
+    if (lane == 0) colbase[c] = mx >= 0 ? (int)(((long long)mn + mx) / 2) : 0;
+}
+
 }  // namespace
 
 cudaError_t launch_validate(const int *rp, const int *ci, int m, int n, int nnz, int *d_err,
@@ -84,6 +121,13 @@ cudaError_t launch_validate(const int *rp, const int *ci, int m, int n, int nnz,
     if (blocks < 1) blocks = 1;
     if (blocks > 65535) blocks = 65535;
     validate_kernel<<<(unsigned)blocks, 256, 0, s>>>(rp, ci, m, n, nnz, d_err);
+    return cudaGetLastError();
+}
+
+cudaError_t chunk_colbase(const Handle &h, const int *rp, const int *ci, cudaStream_t s) {
+    if (h.nchunks <= 0) return cudaSuccess;
+    chunk_colbase_kernel<<<(unsigned)((h.nchunks * 32 + 255) / 256), 256, 0, s>>>(
+        rp, ci, h.arp, h.m, h.nchunks, h.L, h.colbase);
     return cudaGetLastError();
 }
 

@@ -53,6 +53,7 @@ struct Handle {
     void *meta = nullptr;          // per-chunk metadata (CvrMeta or ChunkHdr)
     size_t meta_stride = 0;
     int *tile_ptr = nullptr;       // CSR5 tile -> first row
+    int *colbase = nullptr;        // DELTA16: per-chunk base column of the 16-bit offsets
     double *carry_head = nullptr;  // per-chunk partial of a first row shared with the left
     double *carry_tail = nullptr;  // per-chunk partial of a last row shared with the right
     int *rp = nullptr, *ci = nullptr;  // plain CSR form
@@ -90,6 +91,10 @@ cudaError_t launch_validate(const int *rp, const int *ci, int m, int n, int nnz,
                             cudaStream_t s);
 cudaError_t build_augmented_rowptr(const int *rp, int m, long long padded_total, int *arp,
                                    int *d_nempty, cudaStream_t s);
+
+// DELTA16 base column of every warp chunk (h.colbase): the midpoint of the chunk's smallest
+// and largest column.
+cudaError_t chunk_colbase(const Handle &h, const int *rp, const int *ci, cudaStream_t s);
 
 // Conversions set *ovf (device) to 1 when a 16-bit column offset does not fit.
 cudaError_t cvr_convert(Handle &h, const int *rp, const int *ci, const double *v, int *ovf,

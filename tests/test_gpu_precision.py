@@ -3,7 +3,7 @@
 FP32C: values and x stored in FP32 (the matrices and x are drawn FP32-representable, so the
 oracle's FP64 inputs are the exact widenings), FP32 compensated accumulation, FP64 carries.
 Stated bound: relative error <= 1e-9 per row (cancellation-aware denominator).
-DELTA16: 16-bit column offsets from the chunk's first row; the arithmetic is unchanged, so
+DELTA16: 16-bit column offsets from a per-chunk base column; the arithmetic is unchanged, so
 FP64 + DELTA16 must equal FP64 + I32 bit for bit."""
 import numpy as np
 import pytest
@@ -88,7 +88,8 @@ def test_fp64_delta16_equals_i32(cuda, fmt, kw):
 
 
 def test_delta16_out_of_range_rejected(cuda):
-    A = M.random_csr(50_000, 50_000, 8.0, seed=9)
+    # random columns over 200,000: every chunk spans far more than 65,534 columns
+    A = M.random_csr(50_000, 200_000, 8.0, seed=9)
     with pytest.raises(_abi.PavaError) as e:
         SpMatrix(A, "cvr", index_mode=_abi.INDEX_DELTA16)
     assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
@@ -114,6 +115,27 @@ def test_config3_full_size_fp32c_vs_fp64(cuda):
         bad, mx, mean = O.rel_error(y32, yr, ab, TOL32)
         assert bad == 0, (fmt, mx, mean)
         del m32
+
+
+@pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
+def test_delta16_reaches_any_chunk_of_narrow_column_span(cuda, fmt, kw):
+    """16-bit offsets are taken from each chunk's base column (the middle of its column
+    range): a random 40,000 x 40,000 matrix has columns up to 39,999 away from their row but
+    every chunk spans fewer than 65,535 columns, so it converts with 16-bit offsets; FP64
+    results are bitwise those of 32-bit columns, FP32C within its bound."""
+    torch = cuda
+    A = M.random_csr(40_000, 40_000, 9.0, seed=12)
+    x = M.uniform(A.n, seed=13, fp32=True)
+    A.v = A.v.astype(np.float32).astype(np.float64)
+    xd = torch.from_numpy(x).cuda()
+    d16 = SpMatrix(A, fmt, index_mode=_abi.INDEX_DELTA16, **kw)
+    assert d16.info()["index_mode"] == _abi.INDEX_DELTA16
+    y16 = d16.spmv(xd).cpu().numpy()
+    y32 = SpMatrix(A, fmt, index_mode=_abi.INDEX_I32, **kw).spmv(xd).cpu().numpy()
+    assert np.array_equal(y16, y32)
+    y, _ = _run(torch, A, x, fmt, _abi.PREC_FP32C, _abi.INDEX_AUTO, **kw)
+    yr, ab = O.csr_ref(A.rp, A.ci, A.v, x)
+    assert O.rel_error(y, yr, ab, TOL32)[0] == 0
 
 
 @pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
