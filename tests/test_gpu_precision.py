@@ -139,6 +139,34 @@ def test_delta16_reaches_any_chunk_of_narrow_column_span(cuda, fmt, kw):
 
 
 @pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
+def test_delta16_span_limit(cuda, fmt, kw):
+    """Every row reads the first and the last column, so every chunk spans n - 1 columns:
+    n = 65,535 (span 65,534) fits 16-bit offsets, n = 65,536 does not."""
+    torch = cuda
+    rng = np.random.default_rng(14)
+    for n, fits in ((65_535, True), (65_536, False)):
+        m = 3_000
+        cols = [np.unique(np.concatenate([[0, n - 1], rng.integers(1, n - 1, 6)])) for _ in range(m)]
+        rp = np.concatenate([[0], np.cumsum([len(c) for c in cols])]).astype(np.int32)
+        ci = np.concatenate(cols).astype(np.int32)
+        A = M.from_arrays(m, n, rp, ci, rng.normal(size=len(ci)))
+        if not fits:
+            with pytest.raises(_abi.PavaError) as e:
+                SpMatrix(A, fmt, index_mode=_abi.INDEX_DELTA16, **kw)
+            assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
+            assert SpMatrix(A, fmt, index_mode=_abi.INDEX_AUTO, **kw).info()["index_mode"] == \
+                _abi.INDEX_I32
+            continue
+        xd = torch.from_numpy(M.uniform(n, seed=15)).cuda()
+        d16 = SpMatrix(A, fmt, index_mode=_abi.INDEX_DELTA16, **kw)
+        y16 = d16.spmv(xd).cpu().numpy()
+        y32 = SpMatrix(A, fmt, index_mode=_abi.INDEX_I32, **kw).spmv(xd).cpu().numpy()
+        assert np.array_equal(y16, y32)
+        yr, ab = O.csr_ref(A.rp, A.ci, A.v, xd.cpu().numpy())
+        assert O.rel_error(y16, yr, ab, 1e-12)[0] == 0
+
+
+@pytest.mark.parametrize("fmt,kw", FORMS, ids=FID)
 def test_index_auto_picks_16_bit_where_it_fits(cuda, fmt, kw):
     """PAVA_INDEX_AUTO: 16-bit offsets on a stencil, 32-bit columns when a column is out of
     reach; results bitwise equal to the 32-bit form either way."""
