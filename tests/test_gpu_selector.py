@@ -207,7 +207,7 @@ def test_time_variants_all_run(cuda):
 
 
 def test_selector_regret_on_training_set(cuda):
-    """Trained on the committed timings of 2,000 matrices, judged on the 200 held-out ones:
+    """Trained on the committed timings of 2,000 matrices, evaluated on the 200 held-out ones:
     mean regret vs exhaustive timing <= 10 %, and below the best single fixed variant's."""
     assert os.path.exists(DATA), "tests/golden/selector/selector_timings.npz is missing"
     d = dict(np.load(DATA))
