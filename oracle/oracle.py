@@ -9,7 +9,8 @@ ctypes bindings for the oracle libraries built by oracle/Makefile:
   with an intrinsic shim.  Needs an AVX-512 CPU; ``have_ref()`` says whether it can be used.
 
 Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import this
-module, and only as the checker or the reported CPU baseline.
+module, and only as the oracle the GPU results are compared with or as the reported CPU
+baseline.
 """
 from __future__ import annotations
 

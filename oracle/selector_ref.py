@@ -2,8 +2,8 @@
 
 Only tests/ may import this module; the engine never calls it.  The reference has no
 selector (it runs the formats it is told to), so there is nothing of the reference to pin
-here: these are plain numpy statements of the engine's own definitions, used as the checker
-of the CUDA kernels.
+here: these are plain numpy statements of the engine's own definitions, used as the oracle
+for the CUDA kernels.
 
 * ``features(rp, ci, n)``  -- the 12 structural features of pava_features (float64 here;
   the kernel accumulates the same integer statistics, so they agree to float32 rounding)

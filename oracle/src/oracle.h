@@ -1,8 +1,8 @@
 /*
  * ORACLE -- test infrastructure only.  A plain-C restatement of the reference's CVR and CSR5
  * engines (cvr/cvr.h, csr5/) plus a long-double CSR reference and error metrics.  Only the
- * tests, the smoke check and the CPU-baseline leg of the benchmark use it, as the checker or
- * the reported CPU number; the product never links or calls it.
+ * tests, the smoke check and the CPU-baseline leg of the benchmark use it, as the oracle the
+ * GPU results are compared with or as the reported CPU number; the product never links or calls it.
  *
  * Parity pin: every function here is checked in the CPU test suite against the reference
  * itself, compiled from the reference tree into oracle/_ref (see oracle/Makefile), and against

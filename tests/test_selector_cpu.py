@@ -1,5 +1,5 @@
 """CPU side of the learned selector: the committed training set and the CPU restatement of
-the network used as the checker of the GPU kernels (no GPU needed)."""
+the network used as the oracle for the GPU kernels (no GPU needed)."""
 import os
 
 import numpy as np
