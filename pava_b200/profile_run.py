@@ -8,7 +8,8 @@ of each, for ncu captures and for separating the cost of the x gathers from the 
 Matrices: c1 (512^2 Laplacian), c2 (power-law, 4,194,304 rows), c2local (c2's row lengths and
 values with column j of row r replaced by min(r + j, n-1): the same streams, x gathers that hit
 the same sectors), c3 (128^3 27-point stencil), banded (1,048,576 rows, half-bandwidth 64,
-24 per row).  ``--rows`` shrinks c2 / banded for small captures.  A variant is
+24 per row), batch (the block-diagonal union of ``--count`` of the batching workload's
+matrices, values FP32-representable; 4,096 by default).  ``--rows`` shrinks c2 / banded for small captures.  A variant is
 ``format:key=value;...`` with the pava_opts keys (steps, sigma, tiles_per_chunk, precision
 0=FP64 / 1=FP32C, index_mode 0=I32 / 1=DELTA16, lanes_per_row, col_lanes, cols_per_lane,
 rows_per_tile, x_window).  ``--k K`` (CSR variants) times pava_spmm with K right-hand sides
@@ -23,8 +24,11 @@ import json
 import numpy as np
 
 
-def make_matrix(name, rows):
+def make_matrix(name, rows, count=4096):
     from . import matrices as M
+    if name == "batch":
+        from .batch_bench import batch_mats, union_csr
+        return union_csr(batch_mats(count, fp32=True))
     if name == "c1":
         return M.laplace2d(512)
     if name == "c3":
@@ -60,6 +64,8 @@ def main():
     p.add_argument("--variants", default="cvr:steps=128")
     p.add_argument("--reps", type=int, default=3)
     p.add_argument("--quiet", action="store_true")
+    p.add_argument("--count", type=int, default=4096,
+                   help="matrices in the batch union (--matrix batch)")
     p.add_argument("--k", type=int, default=1,
                    help="right-hand sides: k > 1 times pava_spmm on X (n x k, row-major); "
                         "CSR variants only")
@@ -74,7 +80,7 @@ def main():
 
     torch.cuda.set_device(0)
     _abi.check(_abi.gpu().pava_init(0))
-    A = make_matrix(a.matrix, a.rows)
+    A = make_matrix(a.matrix, a.rows, a.count)
     x64 = M.uniform(A.n, seed=1, fp32=True)
     for fmt, kw in parse_variants(a.variants):
         prec = kw.get("precision", _abi.PREC_FP64)
