@@ -123,6 +123,19 @@ def test_edge_cases(cuda, name, A, fmt, kw):
     _check(y, A, x)
 
 
+@pytest.mark.parametrize("fmt,kw", VARIANTS[:7], ids=VID[:7])
+@pytest.mark.parametrize("name,A", EDGE, ids=[e[0] for e in EDGE])
+def test_edge_cases_16_bit_offsets(cuda, name, A, fmt, kw):
+    """The edge cases with PAVA_INDEX_AUTO (16-bit offsets from each chunk's base column where
+    they reach: empty and all-padding chunks, rows across chunks): bitwise the 32-bit form."""
+    x = M.uniform(A.n, seed=32)
+    y16, mat = _gpu_y(cuda, A, x, fmt, index_mode=_abi.INDEX_AUTO, **kw)
+    y32, _ = _gpu_y(cuda, A, x, fmt, **kw)
+    assert np.array_equal(y16, y32)
+    if A.n <= 65_535:  # every chunk's columns fit a 65,534 span
+        assert mat.info()["index_mode"] == _abi.INDEX_DELTA16
+
+
 def test_empty_rows_are_zero_even_with_nonfinite_x(cuda):
     A = M.from_arrays(4, 3, [0, 1, 1, 2, 2], [0, 2], [2.0, 3.0])
     x = np.array([1.0, np.inf, 2.0])
