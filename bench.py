@@ -466,8 +466,8 @@ def cpu_baseline(A, x, alg):
         from oracle import oracle as O
         ncores = os.cpu_count() or 1
         if O.have_ref():
-            _, conv, per = O.ref_cvr(A.rp, A.ci, A.v, x, nthreads=ncores, iters=10)
-            kind, cores, it = "reference", ncores, 10
+            _, conv, per = O.ref_cvr(A.rp, A.ci, A.v, x, nthreads=ncores, iters=100)
+            kind, cores, it = "reference", ncores, 100
         else:
             _, conv, per = O.cvr_port(A.rp, A.ci, A.v, x, nthreads=ncores, iters=1)
             kind, cores, it = "port", 1, 1
