@@ -113,11 +113,22 @@ typedef struct pava_handle pava_handle;
 /* Selects the CUDA device for the calling thread (cudaSetDevice). */
 pava_status pava_init(int device);
 
+/* Device memory budget of one handle (process-wide setting; 0, the default, means none): a
+ * pava_create whose format arrays would take more than `bytes` fails with PAVA_E_NOMEM and
+ * frees what it allocated, as when the device itself runs out.  The reference sizes nothing
+ * (its arrays are _mm_malloc'd unchecked, cvr/cvr.h:2008-2030).  No GPU needed to set it. */
+pava_status pava_set_device_memory_limit(unsigned long long bytes);
+unsigned long long pava_get_device_memory_limit(void);
+
 /* Converts A into `format` on the device (the GPU form of anonymouslibHandle::inputCSR +
  * asCSR5, csr5/anonymouslib_avx512.h:58-70,107-221, and of CVR's pre_processing,
  * cvr/cvr.h:583-1060).  The caller's arrays are never modified (the reference transposes
  * them in place, format_avx512.h:428).  The conversion is validated first: a row_ptr that
- * is not monotone or a column outside [0, n) gives PAVA_E_INVALID_CSR. */
+ * is not monotone or a column outside [0, n) gives PAVA_E_INVALID_CSR.  Sizes: the CVR and
+ * CSR5 forms index their padded element space with int32, so nnz + 65,600 >= 2^31 (checked
+ * before any array is read) or a padded space past 2^31 - 64 gives PAVA_E_TOO_LARGE, as does
+ * m = 2^31 - 1; a device allocation that fails, or that passes the memory budget of
+ * pava_set_device_memory_limit, gives PAVA_E_NOMEM with nothing left allocated. */
 pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, void *stream,
                         pava_handle **out);
 
@@ -173,7 +184,9 @@ const char *pava_status_string(int status);
  *     the process exits), enough for 32,768 chunks of 4,096 nonzeros: nnz above 134,217,728
  *     returns PAVA_E_TOO_LARGE and launches nothing.
  *   - The first call on a device looks up the array's device address on the current device
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.  The address is
+ *     kept for the life of the process: cudaDeviceReset on that device makes it stale, so a
+ *     process that resets the device must not call this entry point on it again.
  *   - All calls share the array: calls that overlap on the GPU (other streams, other threads)
  *     race and must be serialised by the caller.  Each call rewrites every slot it reads.
  *   - The CSR must be valid (non-decreasing row_ptr, row_ptr[m] == nnz, columns in [0, n)); it
@@ -193,6 +206,12 @@ typedef struct pava_batch pava_batch;
  * columns and nonzeros must stay below 2^31 (PAVA_E_TOO_LARGE). */
 pava_status pava_batch_create(int count, const pava_csr *mats, int format,
                               const pava_opts *opts, void *stream, pava_batch **out);
+/* The same for k right-hand sides per matrix (1 <= k <= 128): format < 0 autotunes the union
+ * for k (pava_autotune over its candidates for k; for k > 1 the CSR row-group shapes), and a
+ * given format must be PAVA_FORMAT_CSR when k > 1.  pava_batch_create is this with k = 1.
+ * The reference's loop runs one matrix and one vector at a time (main.cpp:554-587). */
+pava_status pava_batch_create_spmm(int count, const pava_csr *mats, int k, int format,
+                                   const pava_opts *opts, void *stream, pava_batch **out);
 /* count + 1 prefix offsets of each matrix's x, y and nonzeros in the union (any may be NULL). */
 pava_status pava_batch_layout(const pava_batch *b, long long *x_offsets, long long *y_offsets,
                               long long *nnz_offsets);
@@ -200,9 +219,18 @@ pava_status pava_batch_layout(const pava_batch *b, long long *x_offsets, long lo
 pava_status pava_batch_get(const pava_batch *b, int *format, pava_opts *opts, pava_info *info);
 /* y = U x for the whole batch (x, y device buffers of the union's n and m). */
 pava_status pava_batch_spmv(pava_batch *b, const void *x, void *y, void *stream);
+/* Y = U X for the whole batch with k right-hand sides: X (union n x k) and Y (union m x k)
+ * row-major with leading dimensions ldx, ldy >= k, matrix i's block at rows x_offsets[i] of X
+ * and y_offsets[i] of Y; one persistent launch of the row-group SpMM (CSR-form batches, as
+ * pava_spmm). */
+pava_status pava_batch_spmm(pava_batch *b, int k, const void *X, long long ldx, void *Y,
+                            long long ldy, void *stream);
 /* Records the batch SpMV on (x, y) into a CUDA graph owned by the batch (replacing any
  * earlier one); pava_batch_replay launches it on `stream`. */
 pava_status pava_batch_capture(pava_batch *b, const void *x, void *y);
+/* Records the batch SpMM on (X, Y) into the batch's graph (replacing any earlier one). */
+pava_status pava_batch_capture_spmm(pava_batch *b, int k, const void *X, long long ldx, void *Y,
+                                    long long ldy);
 pava_status pava_batch_replay(pava_batch *b, void *stream);
 pava_status pava_batch_destroy(pava_batch *b);
 
@@ -325,6 +353,27 @@ pava_status pava_coo_to_csr_device(int m, int n, long long nnz, const int *rows,
  * " Performance <name> CVR|CSR5 <SMs> <convert s> <exec s>" (utils/basicMatrix.cpp:491-495).
  * Returns 0 on success or a pava_status.  alpha is accepted and, as in the reference, not
  * applied (cvr/cvr.h never reads it; csr5_spmv_avx512.h comments out its multiply). */
+/* What one benchmark section measured (pava_conduct): the reference prints it as
+ * " Performance ..." and keeps nothing (utils/basicMatrix.cpp:491-495). */
+typedef struct pava_run_record {
+    int status;              /* pava_status of the section */
+    int format, precision, index_mode;
+    int steps, sigma, tiles_per_chunk, lanes_per_row;  /* the form's tile parameters */
+    int sm_count, iterations;
+    long long chunks;
+    double convert_s;        /* device time of the conversion */
+    double exec_s;           /* seconds per timed SpMV (-1 if none ran) */
+    double alg_bytes;        /* compulsory bytes of one SpMV */
+    double format_bytes;     /* bytes one SpMV streams from the format plus x and y */
+} pava_run_record;
+
+/* One benchmark section on a host CSR (the body of conduct_cvr_gpu / conduct_csr5_gpu, for any
+ * format and options): convert, the checked first SpMV into y, `iterations` timed SpMVs, the
+ * Performance line; `rec` (may be NULL) receives the measurements.  opts NULL = the drop-ins'
+ * defaults (16-bit column offsets where they fit). */
+int pava_conduct(int format, const pava_csr *A, const double *x, double *y, const char *name,
+                 int iterations, const pava_opts *opts, pava_run_record *rec);
+
 int conduct_cvr_gpu(int numRows, int numCols, int nItems_raw, int *h_rowDelimiters,
                     int *h_cols, double *h_val, double *h_vec, double *refOut, int alpha,
                     char *matrixName, int numIterations);

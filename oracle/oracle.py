@@ -30,10 +30,17 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _dptr = ctypes.POINTER(ctypes.c_double)
 
 
+def reference_tree() -> str:
+    """The reference's source tree: PAVA_REF, else a `reference` directory beside this
+    repository's own directory."""
+    return os.environ.get("PAVA_REF") or os.path.join(os.path.dirname(os.path.dirname(HERE)),
+                                                      "reference")
+
+
 def build(ref: bool = True) -> None:
     """Builds liboracle.so, and _ref/libpava_ref.so when the reference tree is present."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    ref_tree = os.environ.get("PAVA_REF", "/root/reference")
+    ref_tree = reference_tree()
     if ref and os.path.isfile(os.path.join(ref_tree, "cvr", "cvr.h")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"PAVA_REF={ref_tree}"], check=True)
 

@@ -57,6 +57,14 @@ class PavaInfo(ctypes.Structure):
                 ("alg_bytes", c_dbl), ("format_bytes", c_dbl)]
 
 
+class PavaRunRecord(ctypes.Structure):
+    _fields_ = [("status", c_int), ("format", c_int), ("precision", c_int),
+                ("index_mode", c_int), ("steps", c_int), ("sigma", c_int),
+                ("tiles_per_chunk", c_int), ("lanes_per_row", c_int), ("sm_count", c_int),
+                ("iterations", c_int), ("chunks", c_ll), ("convert_s", c_dbl),
+                ("exec_s", c_dbl), ("alg_bytes", c_dbl), ("format_bytes", c_dbl)]
+
+
 class PavaTuneEntry(ctypes.Structure):
     _fields_ = [("format", c_int), ("opts", PavaOpts), ("ms", c_dbl), ("status", c_int)]
 
@@ -79,6 +87,8 @@ class PavaError(RuntimeError):
 # exported symbols and their prototypes: (name, restype, argtypes)
 GPU_SYMBOLS = [
     ("pava_init", c_int, [c_int]),
+    ("pava_set_device_memory_limit", c_int, [ctypes.c_ulonglong]),
+    ("pava_get_device_memory_limit", ctypes.c_ulonglong, []),
     ("pava_create", c_int, [ctypes.POINTER(PavaCsr), c_int, ctypes.POINTER(PavaOpts), c_void_p,
                             ctypes.POINTER(c_void_p)]),
     ("pava_spmv", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
@@ -95,11 +105,16 @@ GPU_SYMBOLS = [
                                       c_void_p, c_void_p, c_void_p]),
     ("pava_batch_create", c_int, [c_int, ctypes.POINTER(PavaCsr), c_int,
                                   ctypes.POINTER(PavaOpts), c_void_p, ctypes.POINTER(c_void_p)]),
+    ("pava_batch_create_spmm", c_int, [c_int, ctypes.POINTER(PavaCsr), c_int, c_int,
+                                       ctypes.POINTER(PavaOpts), c_void_p,
+                                       ctypes.POINTER(c_void_p)]),
     ("pava_batch_layout", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("pava_batch_get", c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(PavaOpts),
                                ctypes.POINTER(PavaInfo)]),
     ("pava_batch_spmv", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("pava_batch_spmm", c_int, [c_void_p, c_int, c_void_p, c_ll, c_void_p, c_ll, c_void_p]),
     ("pava_batch_capture", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("pava_batch_capture_spmm", c_int, [c_void_p, c_int, c_void_p, c_ll, c_void_p, c_ll]),
     ("pava_batch_replay", c_int, [c_void_p, c_void_p]),
     ("pava_batch_destroy", c_int, [c_void_p]),
     ("pava_autotune", c_int, [ctypes.POINTER(PavaCsr), c_int, c_int, c_int,
@@ -126,6 +141,8 @@ GPU_SYMBOLS = [
                                      ctypes.POINTER(c_void_p), ctypes.POINTER(c_int)]),
     ("pava_coo_to_csr_device", c_int, [c_int, c_int, c_ll, c_void_p, c_void_p, c_void_p, c_int,
                                        c_int, c_void_p, ctypes.POINTER(PavaCsr)]),
+    ("pava_conduct", c_int, [c_int, ctypes.POINTER(PavaCsr), c_void_p, c_void_p, c_char_p, c_int,
+                             ctypes.POINTER(PavaOpts), ctypes.POINTER(PavaRunRecord)]),
     ("conduct_cvr_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_int, c_char_p, c_int]),
     ("conduct_csr5_gpu", c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
@@ -157,6 +174,13 @@ HOST_SYMBOLS = [
                                 c_void_p, c_void_p]),
 ]
 
+PROBE_SYMBOLS = [
+    ("pava_probe_floor", c_int, [c_int, c_void_p, c_void_p, c_void_p, c_ll, c_int, c_u64, c_int,
+                                 c_int, c_void_p, c_void_p]),
+    ("pava_probe_floor_out_len", c_ll, [c_int, c_int]),
+]
+_PROBE = None
+
 
 def _bind(lib, symbols):
     for name, res, args in symbols:
@@ -174,6 +198,10 @@ def gpu_lib_path() -> str:
 
 def host_lib_path() -> str:
     return os.path.join(LIBDIR, "libpava_host.so")
+
+
+def probe_lib_path() -> str:
+    return os.path.join(LIBDIR, "libpava_probe.so")
 
 
 def gpu():
@@ -195,6 +223,17 @@ def host():
             raise ImportError(f"{path} is missing: build it with `python -m pava_b200.build`")
         _HOST = _bind(ctypes.CDLL(path), HOST_SYMBOLS)
     return _HOST
+
+
+def probe():
+    """The floor kernels of include/pava_probe.h (measurement aids, not the product path)."""
+    global _PROBE
+    if _PROBE is None:
+        path = probe_lib_path()
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing: build it with `python -m pava_b200.build`")
+        _PROBE = _bind(ctypes.CDLL(path), PROBE_SYMBOLS)
+    return _PROBE
 
 
 def check(status: int) -> None:

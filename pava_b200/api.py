@@ -194,9 +194,13 @@ class Batch:
 
     ``format`` is 'cvr', 'csr5', 'csr' or 'auto' (autotuned over the candidate forms).  x and
     y of the batch are the matrices' vectors concatenated; ``layout()`` gives the offsets.
+    ``k`` > 1 tunes the batch for k right-hand sides per matrix (``spmm``: X and Y are the
+    matrices' n_i x k and m_i x k blocks stacked, row-major); that takes the 'csr' or 'auto'
+    form.
     """
 
-    def __init__(self, mats, format: str = "auto", precision: int = _abi.PREC_FP64, **opts):
+    def __init__(self, mats, format: str = "auto", precision: int = _abi.PREC_FP64, k: int = 1,
+                 **opts):
         keep = []
         arr = (_abi.PavaCsr * len(mats))()
         for i, A in enumerate(mats):
@@ -207,9 +211,10 @@ class Batch:
             setattr(o, key, val)
         fmt = -1 if format == "auto" else FORMATS[format]
         h = _abi.c_void_p()
-        _abi.check(_abi.gpu().pava_batch_create(len(mats), arr, fmt, ctypes.byref(o), None,
-                                                ctypes.byref(h)))
+        _abi.check(_abi.gpu().pava_batch_create_spmm(len(mats), arr, k, fmt, ctypes.byref(o),
+                                                     None, ctypes.byref(h)))
         self._h = h
+        self.k = k
         self.count = len(mats)
         self.precision = precision
         xo = np.zeros(self.count + 1, np.int64)
@@ -252,6 +257,34 @@ class Batch:
         self._check_xy(x, y)
         self._graph_xy = (x, y)
         _abi.check(_abi.gpu().pava_batch_capture(self._h, x.data_ptr(), y.data_ptr()))
+
+    def _check_XY(self, X, Y):
+        torch = _torch()
+        want = torch.float32 if self.precision == _abi.PREC_FP32C else torch.float64
+        if X.dim() != 2 or X.dtype != want or not X.is_cuda or X.shape[0] < self.n or X.stride(1) != 1:
+            raise TypeError(f"X must be a CUDA {want} matrix of {self.n} row-major rows")
+        if (Y.dim() != 2 or Y.dtype != torch.float64 or not Y.is_cuda or Y.shape[0] < self.m
+                or Y.stride(1) != 1 or Y.shape[1] != X.shape[1]):
+            raise TypeError(f"Y must be a CUDA float64 matrix of {self.m} row-major rows and "
+                            "X's columns")
+
+    def spmm(self, X, Y=None, stream=None):
+        """Y = U X for the whole batch: X stacks the matrices' n_i x k right-hand sides."""
+        torch = _torch()
+        if Y is None:
+            Y = torch.empty((self.m, X.shape[1]), dtype=torch.float64, device=X.device)
+        self._check_XY(X, Y)
+        _abi.check(_abi.gpu().pava_batch_spmm(self._h, X.shape[1], X.data_ptr(), X.stride(0),
+                                              Y.data_ptr(), Y.stride(0),
+                                              _abi.c_void_p(_stream_ptr(stream))))
+        return Y
+
+    def capture_spmm(self, X, Y):
+        """Records the SpMM on (X, Y) into the batch's CUDA graph."""
+        self._check_XY(X, Y)
+        self._graph_xy = (X, Y)
+        _abi.check(_abi.gpu().pava_batch_capture_spmm(self._h, X.shape[1], X.data_ptr(),
+                                                      X.stride(0), Y.data_ptr(), Y.stride(0)))
 
     def replay(self, stream=None):
         _abi.check(_abi.gpu().pava_batch_replay(self._h, _abi.c_void_p(_stream_ptr(stream))))

@@ -12,6 +12,8 @@ graph, and a banded matrix with k right-hand sides; forms picked by the autotune
 * banded: 1,048,576 rows, half-bandwidth 64, 24 distinct columns per row, X row-major n x k
   for k in {1, 8, 32}; the CSR row-group shape (lanes per row, lanes across k, columns per
   lane, rows per tile) is autotuned per k.
+* batch_spmm: the 4,096-matrix batch with k in {8, 32} right-hand sides per matrix, autotuned
+  for k, one persistent launch captured into a CUDA graph and replayed.
 
 Each line is one JSON object: device time per product (CUDA events, median of --reps after
 warm-up; every input is larger than the 126 MB L2 except where noted), the compulsory
@@ -123,6 +125,31 @@ def run_batch(torch, count, reps, peak, precision):
             "create_s": create_s, "autotune": table}
 
 
+def run_batch_spmm(torch, count, k, reps, peak):
+    """The 4,096-matrix batch with k right-hand sides per matrix (X_i n_i x k, row-major,
+    U[-1, 1]): autotuned for k, captured into a CUDA graph, replayed."""
+    mats = batch_mats(count)
+    t0 = time.time()
+    b = Batch(mats, "auto", k=k)
+    create_s = time.time() - t0
+    fmt, opts = b.chosen()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(100 + k)
+    X = torch.rand((b.n, k), generator=g, dtype=torch.float64, device="cuda") * 2.0 - 1.0
+    Y = torch.empty((b.m, k), dtype=torch.float64, device="cuda")
+    b.capture_spmm(X, Y)
+    ms, _ = time_it(torch, lambda: b.replay(), reps)
+    Yr = Y.clone()
+    b.spmm(X, Y)
+    assert torch.equal(Y, Yr), "graph replay differs from a launch"
+    alg = b.nnz * 12 + 4 * (b.m + count) + 8 * b.n * k + 8 * b.m * k
+    gbs = alg / (ms * 1e-3) / 1e9
+    return {"workload": "batch_spmm", "matrices": count, "rows": b.m, "nnz": b.nnz, "k": k,
+            "precision": "fp64", "form": fmt, "opts": {kk: v for kk, v in opts.items() if v},
+            "launch": "cuda graph replay (one persistent launch)", "ms": ms, "alg_bytes": alg,
+            "GBps": gbs, "frac_hbm": gbs / peak[0], "peak": peak[1], "create_s": create_s}
+
+
 def run_banded(torch, rows, ks, reps, peak):
     A = M.banded(rows, 64, 24, seed=3)
     out = []
@@ -157,7 +184,7 @@ def run_banded(torch, rows, ks, reps, peak):
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("--only", choices=["batch", "banded"], default=None)
+    p.add_argument("--only", choices=["batch", "banded", "batch_spmm"], default=None)
     p.add_argument("--count", type=int, default=4096)
     p.add_argument("--rows", type=int, default=1_048_576)
     p.add_argument("--reps", type=int, default=20)
@@ -172,6 +199,9 @@ def main():
     if a.only in (None, "batch"):
         for prec in (_abi.PREC_FP64, _abi.PREC_FP32C):
             print(json.dumps(run_batch(torch, a.count, a.reps, peak, prec)), flush=True)
+    if a.only in (None, "batch_spmm"):
+        for k in (8, 32):
+            print(json.dumps(run_batch_spmm(torch, a.count, k, a.reps, peak)), flush=True)
 
 
 if __name__ == "__main__":

@@ -6,6 +6,7 @@
 * ``pava_b200/lib/libpava_host.so`` -- host-side C++: seeded matrix generators, the Matrix
   Market reader/writer and the COO->CSR conversion (include/pava_host.h)
 * ``pava_b200/lib/pava_bench``      -- main.cpp's CVR / CSR5 benchmark loop over the C ABI
+* ``pava_b200/lib/libpava_probe.so`` -- floor kernels for measurements (include/pava_probe.h)
 
 nvcc cross-compiles for sm_100a without a GPU, so this runs on any machine with the CUDA
 toolkit.  CUDA runtime is linked statically, so the library does not depend on the
@@ -16,6 +17,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -41,25 +43,33 @@ def _stale(target, sources):
     return any(os.path.getmtime(s) > t for s in sources)
 
 
-def build_gpu(force: bool = False, verbose_ptxas: bool = False) -> str:
+def build_gpu(force: bool = False, verbose_ptxas: bool = False, out: str | None = None,
+              extra: tuple = ()) -> str:
+    """libpava_gpu.so; `out` and `extra` (nvcc flags such as -D macros) build a variant of it
+    elsewhere, e.g. with other launch bounds for a tuning sweep (loaded through PAVA_GPU_LIB)."""
     os.makedirs(LIBDIR, exist_ok=True)
-    out = os.path.join(LIBDIR, "libpava_gpu.so")
+    out = out or os.path.join(LIBDIR, "libpava_gpu.so")
     srcs = [os.path.join(CSRC, s) for s in GPU_SOURCES]
     deps = srcs + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     deps.append(os.path.join(ROOT, "include", "pava_gpu.h"))
     if not force and not _stale(out, deps):
         return out
-    objdir = os.path.join(LIBDIR, "obj")
+    objdir = os.path.join(os.path.dirname(out), "obj" if not extra else
+                          "obj_" + os.path.splitext(os.path.basename(out))[0])
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for s in srcs:
         o = os.path.join(objdir, os.path.basename(s) + ".o")
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-               "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-c", s, "-o", o]
+               "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), *extra,
+               "-c", s, "-o", o]
         if verbose_ptxas:
             cmd.insert(1, "-Xptxas=-v")
-        _run(cmd)
+        cmds.append(cmd)
         objs.append(o)
+    # the translation units compile independently: one nvcc per core
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(_run, cmds))
     _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", out, *objs])
     return out
 
@@ -89,9 +99,25 @@ def build_driver(force: bool = False) -> str:
     return out
 
 
+def build_probe(force: bool = False) -> str:
+    """libpava_probe.so: the floor kernels of include/pava_probe.h (measurement aids)."""
+    os.makedirs(LIBDIR, exist_ok=True)
+    out = os.path.join(LIBDIR, "libpava_probe.so")
+    src = os.path.join(CSRC, "k_probe.cu")
+    deps = [src, os.path.join(CSRC, "pava_common.cuh"), os.path.join(ROOT, "include", "pava_probe.h")]
+    if not force and not _stale(out, deps):
+        return out
+    _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+          "-cudart", "static", "-o", out, src])
+    return out
+
+
 def build(force: bool = False) -> None:
-    build_host(force)
-    build_gpu(force)
+    with ThreadPoolExecutor(max_workers=2) as ex:
+        fp = ex.submit(build_probe, force)
+        build_host(force)
+        build_gpu(force)
+        fp.result()
     build_driver(force)
 
 

@@ -4,6 +4,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
 #include <climits>
 #include <string>
 
@@ -83,13 +84,24 @@ pava_status fail_cuda(cudaError_t e, const char *where) {
         if (e_ != cudaSuccess) return fail_cuda(e_, where);  \
     } while (0)
 
+// Bytes of device memory one handle may hold (0: no limit), pava_set_device_memory_limit.
+std::atomic<unsigned long long> g_mem_limit{0};
+
+// A handle's device allocation: counted in *acc and refused, as an allocation failure, when it
+// would take the handle past the memory limit.
+cudaError_t budget_malloc(void **p, size_t bytes, size_t *acc) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 1;
+    const unsigned long long lim = g_mem_limit.load();
+    if (lim && acc && (unsigned long long)*acc + bytes > lim) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess && acc) *acc += bytes;
+    return e;
+}
+
 template <typename T>
 cudaError_t dalloc(T **p, size_t count, size_t *acc) {
-    *p = nullptr;
-    if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * count);
-    if (e == cudaSuccess && acc) *acc += sizeof(T) * count;
-    return e;
+    return budget_malloc((void **)p, sizeof(T) * (count ? count : 1), acc);
 }
 
 void free_handle_buffers(pava::Handle &h) {
@@ -202,10 +214,10 @@ pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double 
         pava_status st = plan_chunks(h, rp, s);
         if (st != PAVA_SUCCESS) return st;
         const size_t padded = (size_t)(h.nchunks * h.L);
-        PAVA_CUDA(cudaMalloc(&h.vals, sv * (padded ? padded : 1)), "cudaMalloc(vals)");
-        h.device_bytes += sv * padded;
-        PAVA_CUDA(cudaMalloc(&h.cols, si * (padded ? padded : 1)), "cudaMalloc(cols)");
-        h.device_bytes += si * padded;
+        PAVA_CUDA(budget_malloc(&h.vals, sv * (padded ? padded : 1), &h.device_bytes),
+                  "cudaMalloc(vals)");
+        PAVA_CUDA(budget_malloc(&h.cols, si * (padded ? padded : 1), &h.device_bytes),
+                  "cudaMalloc(cols)");
         PAVA_CUDA(dalloc(&h.carry_head, (size_t)h.nchunks, &h.device_bytes), "cudaMalloc(carry)");
         PAVA_CUDA(dalloc(&h.carry_tail, (size_t)h.nchunks, &h.device_bytes), "cudaMalloc(carry)");
         if (h.index_mode == PAVA_INDEX_DELTA16) {
@@ -243,8 +255,7 @@ pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double 
         PAVA_CUDA(dalloc(&h.rp, (size_t)h.m + 1, &h.device_bytes), "cudaMalloc(rp)");
         PAVA_CUDA(dalloc(&h.ci, (size_t)h.nnz, &h.device_bytes), "cudaMalloc(ci)");
         const size_t nv = (size_t)(h.nnz ? h.nnz : 1);
-        PAVA_CUDA(cudaMalloc(&h.v, sv * nv), "cudaMalloc(v)");
-        h.device_bytes += sv * nv;
+        PAVA_CUDA(budget_malloc(&h.v, sv * nv, &h.device_bytes), "cudaMalloc(v)");
         PAVA_CUDA(cudaMemcpyAsync(h.rp, rp, sizeof(int) * ((size_t)h.m + 1),
                                   cudaMemcpyDeviceToDevice, s), "copy rp");
         if (h.nnz > 0) {
@@ -269,6 +280,13 @@ void set_last_error(const std::string &msg) { g_last_error = msg; }
 }  // namespace pava
 
 extern "C" {
+
+pava_status pava_set_device_memory_limit(unsigned long long bytes) {
+    g_mem_limit.store(bytes);
+    return PAVA_SUCCESS;
+}
+
+unsigned long long pava_get_device_memory_limit(void) { return g_mem_limit.load(); }
 
 pava_status pava_init(int device) {
     int count = 0;
@@ -313,6 +331,14 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
     pava_opts o;
     memset(&o, 0, sizeof(o));
     if (opts) o = *opts;
+    // sizes that cannot fit the int32 element space of the chunked forms, however few rows are
+    // empty (the largest chunk is 32 x 32 x 64 elements): refused before any array is read
+    if (format != PAVA_FORMAT_CSR && (long long)A->nnz + 65536 >= (long long)INT_MAX - 64)
+        return fail(PAVA_E_TOO_LARGE, "nnz " + std::to_string(A->nnz) +
+                                          " leaves no room for chunk padding in the int32 "
+                                          "element space");
+    if (A->m == INT_MAX)  // m + 1 row pointers and the padding row must be indexable
+        return fail(PAVA_E_TOO_LARGE, "m must be below 2^31 - 1");
     if (o.precision != PAVA_PREC_FP64 && o.precision != PAVA_PREC_FP32C)
         return fail(PAVA_E_UNSUPPORTED_VALUE_TYPE, "unknown precision");
     if (o.index_mode != PAVA_INDEX_I32 && o.index_mode != PAVA_INDEX_DELTA16 &&
@@ -607,15 +633,24 @@ pava_status pava_destroy(pava_handle *H) {
 namespace {
 
 int conduct_gpu(int format, int m, int n, int nnz, const int *rp, const int *ci,
-                const double *v, const double *x, double *y, const char *name, int iters) {
+                const double *v, const double *x, double *y, const char *name, int iters,
+                const pava_opts *opts, pava_run_record *rec) {
     pava_csr A{m, n, nnz, rp, ci, v, 0};
     pava_handle *H = nullptr;
     pava_opts o;
     memset(&o, 0, sizeof(o));
-    o.index_mode = PAVA_INDEX_AUTO;  // 16-bit column offsets where they fit: same results
+    if (opts) o = *opts;
+    else o.index_mode = PAVA_INDEX_AUTO;  // 16-bit column offsets where they fit: same results
+    if (rec) {
+        memset(rec, 0, sizeof(*rec));
+        rec->status = PAVA_E_INVALID_ARG;
+        rec->convert_s = rec->exec_s = -1.0;
+    }
+    const char *fname = format == PAVA_FORMAT_CVR ? "CVR" : (format == PAVA_FORMAT_CSR5 ? "CSR5" : "CSR");
     int st = pava_create(&A, format, &o, nullptr, &H);
     if (st != PAVA_SUCCESS) {
-        printf(" Performance %s %s %d %f %f \n", name ? name : "", format == PAVA_FORMAT_CVR ? "CVR" : "CSR5", 0, -1.0, -1.0);
+        printf(" Performance %s %s %d %f %f \n", name ? name : "", fname, 0, -1.0, -1.0);
+        if (rec) rec->status = st;
         return st;
     }
     // the checked first call, then the timed calls (cvr/cvr.h:2108-2112; csr5/csr5.h:149-153)
@@ -636,21 +671,52 @@ int conduct_gpu(int format, int m, int n, int nnz, const int *rp, const int *ci,
         cudaEventDestroy(a);
         cudaEventDestroy(b);
     }
-    printf(" Performance %s %s %d %f %f \n", name ? name : "", format == PAVA_FORMAT_CVR ? "CVR" : "CSR5",
-           H->h.sm_count, H->h.convert_ms * 1e-3, exec_s);
+    printf(" Performance %s %s %d %f %f \n", name ? name : "", fname, H->h.sm_count,
+           H->h.convert_ms * 1e-3, exec_s);
     fflush(stdout);
+    if (rec) {
+        const pava::Handle &h = H->h;
+        pava_info inf;
+        pava_get_info(H, &inf);
+        rec->status = st;
+        rec->format = h.format;
+        rec->precision = h.precision;
+        rec->index_mode = h.index_mode;
+        rec->steps = h.S;
+        rec->sigma = h.sigma;
+        rec->tiles_per_chunk = h.G;
+        rec->lanes_per_row = h.lanes_per_row;
+        rec->sm_count = h.sm_count;
+        rec->iterations = iters;
+        rec->chunks = h.nchunks;
+        rec->convert_s = h.convert_ms * 1e-3;
+        rec->exec_s = exec_s;
+        rec->alg_bytes = inf.alg_bytes;
+        rec->format_bytes = inf.format_bytes;
+    }
     pava_destroy(H);
     return st;
 }
 
 }  // namespace
 
+extern "C" int pava_conduct(int format, const pava_csr *A, const double *x, double *y,
+                            const char *name, int iterations, const pava_opts *opts,
+                            pava_run_record *rec) {
+    if (!A || A->on_device || !x || !y) {
+        g_last_error = "pava_conduct: host CSR, x and y required";
+        return PAVA_E_INVALID_ARG;
+    }
+    return conduct_gpu(format, A->m, A->n, A->nnz, A->row_ptr, A->col_idx, A->vals, x, y, name,
+                       iterations, opts, rec);
+}
+
 extern "C" int conduct_cvr_gpu(int numRows, int numCols, int nItems_raw, int *h_rowDelimiters,
                                int *h_cols, double *h_val, double *h_vec, double *refOut,
                                int alpha, char *matrixName, int numIterations) {
     (void)alpha;
     return conduct_gpu(PAVA_FORMAT_CVR, numRows, numCols, nItems_raw, h_rowDelimiters, h_cols,
-                       h_val, h_vec, refOut, matrixName, numIterations);
+                       h_val, h_vec, refOut, matrixName, numIterations, nullptr, nullptr);
 }
 
 extern "C" int conduct_csr5_gpu(int m, int n, int nnzA, int *csrRowPtrA, int *csrColIdxA,
@@ -658,5 +724,5 @@ extern "C" int conduct_csr5_gpu(int m, int n, int nnzA, int *csrRowPtrA, int *cs
                                 char *matrixName, int numIterations) {
     (void)alpha;
     return conduct_gpu(PAVA_FORMAT_CSR5, m, n, nnzA, csrRowPtrA, csrColIdxA, csrValA, x, y,
-                       matrixName, numIterations);
+                       matrixName, numIterations, nullptr, nullptr);
 }

@@ -4,8 +4,10 @@
 // and nonzeros concatenated, column indices shifted by the matrix's column offset.  Then
 // [y_0; ...; y_{N-1}] = U [x_0; ...; x_{N-1}] is one SpMV over the union, so the whole batch is
 // one launch of any engine form, uneven sizes included; with the row-group form that launch
-// is persistent (grid = resident capacity, warps take row tiles).  A batch can record its SpMV
-// into a CUDA graph once and replay it.
+// is persistent (grid = resident capacity, warps take row tiles).  With k right-hand sides per
+// matrix (X_i row-major n_i x k, stacked into the union's n x k X) the same union gives
+// [Y_0; ...; Y_{N-1}] = U X in one persistent launch of the row-group SpMM.  A batch can record
+// its SpMV or SpMM into a CUDA graph once and replay it.
 //
 // The autotuner converts a matrix into every candidate form and times it with CUDA events:
 // it is the exhaustive search that picks tiles and lanes per row, and the measure of the
@@ -24,6 +26,7 @@ struct pava_batch {
     int precision = 0;
     std::vector<long long> row_off, col_off, nnz_off;  // count + 1 prefix offsets
     pava_handle *inner = nullptr;                      // the union in the chosen form
+    int k = 1;                                         // right-hand sides it was tuned for
     int format = 0;
     pava_opts opts{};
     cudaGraph_t graph = nullptr;
@@ -308,14 +311,18 @@ pava_status pava_autotune(const pava_csr *A, int k, int precision, int reps,
     return PAVA_SUCCESS;
 }
 
-pava_status pava_batch_create(int count, const pava_csr *mats, int format, const pava_opts *opts,
-                              void *stream, pava_batch **out) {
+pava_status pava_batch_create_spmm(int count, const pava_csr *mats, int k, int format,
+                                   const pava_opts *opts, void *stream, pava_batch **out) {
     if (!out) return bfail(PAVA_E_INVALID_ARG, "out is NULL");
     *out = nullptr;
     if (count < 1 || !mats) return bfail(PAVA_E_INVALID_ARG, "empty batch");
+    if (k < 1 || k > 128) return bfail(PAVA_E_INVALID_ARG, "k must be in [1, 128]");
+    if (k > 1 && format >= 0 && format != PAVA_FORMAT_CSR)
+        return bfail(PAVA_E_UNKNOWN_FORMAT, "k > 1 right-hand sides need the CSR row-group form");
     pava_batch *b = new (std::nothrow) pava_batch();
     if (!b) return bfail(PAVA_E_NOMEM, "host allocation failed");
     b->count = count;
+    b->k = k;
     pava_opts o;
     memset(&o, 0, sizeof(o));
     if (opts) o = *opts;
@@ -326,10 +333,10 @@ pava_status pava_batch_create(int count, const pava_csr *mats, int format, const
     if (st != PAVA_SUCCESS) { delete b; return st; }
     pava_csr U{(int)b->row_off[count], (int)b->col_off[count], (int)b->nnz_off[count], u.rp,
                u.ci, u.v, 1};
-    if (format < 0) {  // autotune over the built-in candidates (k = 1)
-        std::vector<pava_tune_entry> ent(64);
+    if (format < 0) {  // autotune over the built-in candidates for k right-hand sides
+        std::vector<pava_tune_entry> ent(128);
         int ne = 0, bi = -1;
-        st = pava_autotune(&U, 1, o.precision, 5, ent.data(), (int)ent.size(), &ne, &bi);
+        st = pava_autotune(&U, k, o.precision, 5, ent.data(), (int)ent.size(), &ne, &bi);
         if (st != PAVA_SUCCESS) { u.release(); delete b; return st; }
         format = ent[bi].format;
         o = ent[bi].opts;
@@ -344,6 +351,11 @@ pava_status pava_batch_create(int count, const pava_csr *mats, int format, const
     }
     *out = b;
     return PAVA_SUCCESS;
+}
+
+pava_status pava_batch_create(int count, const pava_csr *mats, int format, const pava_opts *opts,
+                              void *stream, pava_batch **out) {
+    return pava_batch_create_spmm(count, mats, 1, format, opts, stream, out);
 }
 
 pava_status pava_batch_layout(const pava_batch *b, long long *x_offsets, long long *y_offsets,
@@ -369,8 +381,20 @@ pava_status pava_batch_spmv(pava_batch *b, const void *x, void *y, void *stream)
     return pava_spmv(b->inner, x, y, stream);
 }
 
-pava_status pava_batch_capture(pava_batch *b, const void *x, void *y) {
+pava_status pava_batch_spmm(pava_batch *b, int k, const void *X, long long ldx, void *Y,
+                            long long ldy, void *stream) {
     if (!b) return bfail(PAVA_E_INVALID_ARG, "batch is NULL");
+    return pava_spmm(b->inner, k, X, ldx, Y, ldy, stream);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Records one product on the batch's capture stream into the batch's graph (replacing any
+// earlier one); `run` issues the launches on the stream it is given.
+template <typename F>
+pava_status capture_into(pava_batch *b, F run) {
     if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
     cudaError_t e = cudaSuccess;
@@ -378,7 +402,7 @@ pava_status pava_batch_capture(pava_batch *b, const void *x, void *y) {
     if (e == cudaSuccess) e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess)
         return bfail(PAVA_E_CUDA, std::string("begin capture: ") + cudaGetErrorString(e));
-    pava_status st = pava_spmv(b->inner, x, y, b->cap_stream);
+    pava_status st = run(b->cap_stream);
     e = cudaStreamEndCapture(b->cap_stream, &b->graph);
     if (st != PAVA_SUCCESS) {
         if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
@@ -388,6 +412,22 @@ pava_status pava_batch_capture(pava_batch *b, const void *x, void *y) {
     if (e != cudaSuccess)
         return bfail(PAVA_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     return PAVA_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+pava_status pava_batch_capture(pava_batch *b, const void *x, void *y) {
+    if (!b) return bfail(PAVA_E_INVALID_ARG, "batch is NULL");
+    return capture_into(b, [&](cudaStream_t cs) { return pava_spmv(b->inner, x, y, cs); });
+}
+
+pava_status pava_batch_capture_spmm(pava_batch *b, int k, const void *X, long long ldx, void *Y,
+                                    long long ldy) {
+    if (!b) return bfail(PAVA_E_INVALID_ARG, "batch is NULL");
+    return capture_into(
+        b, [&](cudaStream_t cs) { return pava_spmm(b->inner, k, X, ldx, Y, ldy, cs); });
 }
 
 pava_status pava_batch_replay(pava_batch *b, void *stream) {

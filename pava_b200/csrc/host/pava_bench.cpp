@@ -11,6 +11,13 @@
 // reference's check counts rows off by more than 1 % of y_ref (checkResults,
 // basicMatrix.cpp:559-587) against a serial CSR product (referenceSpMV, :538-556).  The CVR
 // section keeps main.cpp's guard of both dimensions above 4096 (main.cpp:558).
+//
+// Beside each Performance line the driver prints one machine-readable record, a JSON object on
+// a line of its own starting with {"record": "pava_bench": the section's form and tile
+// parameters, convert and exec seconds, GB/s by the compulsory byte model and its fraction of
+// the HBM peak (PAVA_HBM_PEAK_GBS, else MEASURED_PEAKS.json two directories above the
+// executable, else 6,650 GB/s marked "fallback"), and the error of y against the serial product
+// (per-row relative error with the cancellation-aware denominator max(|y_ref|, sum |a x|)).
 
 #include <math.h>
 #include <stdio.h>
@@ -35,12 +42,82 @@ int check_results(int m, const double *y, const double *y_ref) {
 }
 
 void reference_spmv(int m, const int *rp, const int *ci, const double *v, const double *x,
-                    double *y) {
+                    double *y, double *absum) {
     for (int r = 0; r < m; ++r) {
-        double s = 0.0;
-        for (int j = rp[r]; j < rp[r + 1]; ++j) s += v[j] * x[ci[j]];
+        double s = 0.0, a = 0.0;
+        for (int j = rp[r]; j < rp[r + 1]; ++j) {
+            s += v[j] * x[ci[j]];
+            a += fabs(v[j] * x[ci[j]]);
+        }
         y[r] = s;
+        absum[r] = a;
     }
+}
+
+struct Peak {
+    double gbs = 6650.0;
+    const char *kind = "fallback";
+};
+
+// The HBM peak the roofline fraction is taken against.
+Peak hbm_peak(const char *argv0) {
+    Peak p;
+    if (const char *env = getenv("PAVA_HBM_PEAK_GBS")) {
+        p.gbs = atof(env);
+        p.kind = "env";
+        return p;
+    }
+    std::string dir(argv0);
+    const size_t slash = dir.find_last_of('/');
+    dir = slash == std::string::npos ? std::string(".") : dir.substr(0, slash);
+    FILE *f = fopen((dir + "/../../MEASURED_PEAKS.json").c_str(), "r");
+    if (!f) return p;
+    std::string text;
+    char buf[4096];
+    size_t got;
+    while ((got = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
+    fclose(f);
+    const size_t k = text.find("\"hbm_gbs\"");
+    if (k != std::string::npos) {
+        const size_t colon = text.find(':', k);
+        if (colon != std::string::npos) {
+            const double v = atof(text.c_str() + colon + 1);
+            if (v > 0) {
+                p.gbs = v;
+                p.kind = "measured";
+            }
+        }
+    }
+    return p;
+}
+
+void print_record(const std::string &name, const char *section, const pava_run_record &r, int m,
+                  int n, int nnz, const double *y, const double *y_ref, const double *absum,
+                  int rows_off, const Peak &peak) {
+    double mx = 0.0, mean = 0.0;
+    for (int i = 0; i < m; ++i) {
+        double den = fabs(y_ref[i]) > absum[i] ? fabs(y_ref[i]) : absum[i];
+        if (den < 1e-300) den = 1e-300;
+        const double e = fabs(y[i] - y_ref[i]) / den;
+        mx = e > mx ? e : mx;
+        mean += e;
+    }
+    mean = m ? mean / m : 0.0;
+    const double gbs = r.exec_s > 0 ? r.alg_bytes / r.exec_s / 1e9 : -1.0;
+    printf("{\"record\": \"pava_bench\", \"matrix\": \"%s\", \"section\": \"%s\", "
+           "\"status\": %d, \"m\": %d, \"n\": %d, \"nnz\": %d, \"format\": %d, "
+           "\"precision\": %d, \"index_bytes\": %d, \"steps\": %d, \"sigma\": %d, "
+           "\"tiles_per_chunk\": %d, \"chunks\": %lld, \"sms\": %d, \"iterations\": %d, "
+           "\"convert_s\": %.6e, \"exec_s\": %.6e, \"alg_bytes\": %.0f, "
+           "\"format_bytes\": %.0f, \"GBps\": %.3f, \"peak_GBps\": %.1f, "
+           "\"peak_kind\": \"%s\", \"roofline_frac\": %.4f, \"max_rel_err\": %.3e, "
+           "\"mean_rel_err\": %.3e, \"rows_off_1pct\": %d}\n",
+           name.c_str(), section, r.status, m, n, nnz, r.format, r.precision,
+           r.index_mode == PAVA_INDEX_DELTA16 ? 2 : 4, r.steps, r.sigma, r.tiles_per_chunk,
+           r.chunks, r.sm_count, r.iterations, r.convert_s, r.exec_s, r.alg_bytes,
+           r.format_bytes, gbs, peak.gbs, peak.kind, gbs > 0 ? gbs / peak.gbs : -1.0, mx, mean,
+           rows_off);
+    fflush(stdout);
 }
 
 struct Csr {
@@ -120,9 +197,15 @@ int main(int argc, char **argv) {
         return 1;
     }
     const int nnz = A.rp[A.m];
-    std::vector<double> x(A.n), y(A.m), y_ref(A.m);
+    std::vector<double> x(A.n), y(A.m), y_ref(A.m), absum(A.m);
     pava_init_vectors(A.m, A.n, x.data(), y.data(), y_ref.data());
-    reference_spmv(A.m, A.rp.data(), A.ci.data(), A.v.data(), x.data(), y_ref.data());
+    reference_spmv(A.m, A.rp.data(), A.ci.data(), A.v.data(), x.data(), y_ref.data(),
+                   absum.data());
+    const Peak peak = hbm_peak(argv[0]);
+    const pava_csr csr{A.m, A.n, nnz, A.rp.data(), A.ci.data(), A.v.data(), 0};
+    pava_opts opts;
+    memset(&opts, 0, sizeof(opts));
+    opts.index_mode = PAVA_INDEX_AUTO;  // what conduct_cvr_gpu / conduct_csr5_gpu use
     printf("matrix %s: %d x %d, %d nonzeros\n", name.c_str(), A.m, A.n, nnz);
     std::vector<char> cname(name.begin(), name.end());
     cname.push_back('\0');
@@ -131,20 +214,26 @@ int main(int argc, char **argv) {
     printf("**************\n      CVR      \n**************\n");
     if (A.m > 4096 && A.n > 4096) {
         pava_init_vectors(A.m, A.n, nullptr, y.data(), nullptr);
-        const int st = conduct_cvr_gpu(A.m, A.n, nnz, A.rp.data(), A.ci.data(), A.v.data(),
-                                       x.data(), y.data(), 1, cname.data(), iters);
+        pava_run_record rec;
+        const int st = pava_conduct(PAVA_FORMAT_CVR, &csr, x.data(), y.data(), cname.data(),
+                                    iters, &opts, &rec);
         const int bad = check_results(A.m, y.data(), y_ref.data());
         printf("CVR status %d, rows off by more than 1%%: %d\n", st, bad);
+        print_record(name, "CVR", rec, A.m, A.n, nnz, y.data(), y_ref.data(), absum.data(), bad,
+                     peak);
         failures += (st != 0) + (bad != 0);
     } else {
         printf(" Performance %s %s %d %f %f \n", cname.data(), "CVR", 0, -1.0, -1.0);
     }
     printf("**************\n     CSR5     \n**************\n");
     pava_init_vectors(A.m, A.n, nullptr, y.data(), nullptr);
-    const int st = conduct_csr5_gpu(A.m, A.n, nnz, A.rp.data(), A.ci.data(), A.v.data(),
-                                    x.data(), y.data(), 1.0, cname.data(), iters);
+    pava_run_record rec;
+    const int st = pava_conduct(PAVA_FORMAT_CSR5, &csr, x.data(), y.data(), cname.data(), iters,
+                                &opts, &rec);
     const int bad = check_results(A.m, y.data(), y_ref.data());
     printf("CSR5 status %d, rows off by more than 1%%: %d\n", st, bad);
+    print_record(name, "CSR5", rec, A.m, A.n, nnz, y.data(), y_ref.data(), absum.data(), bad,
+                 peak);
     failures += (st != 0) + (bad != 0);
     return failures ? 1 : 0;
 }

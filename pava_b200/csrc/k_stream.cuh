@@ -148,14 +148,16 @@ template <> struct Acc<float> {
         return (double)v.x + (double)v.y;
     }
     float s = 0.f, c = 0.f;
+    // Every step rounds on its own (the _rn intrinsics are never contracted into an FMA),
+    // which the exactness of TwoProduct and TwoSum relies on.
     __device__ __forceinline__ void add(float v, float x) {
-        const float p = v * x;
-        const float e = fmaf(v, x, -p);  // v*x = p + e exactly
-        const float t = s + p;           // TwoSum(s, p) = t + err exactly
-        const float z = t - s;
-        const float err = (s - (t - z)) + (p - z);
+        const float p = __fmul_rn(v, x);
+        const float e = __fmaf_rn(v, x, -p);  // v*x = p + e exactly
+        const float t = __fadd_rn(s, p);      // TwoSum(s, p) = t + err exactly
+        const float z = __fsub_rn(t, s);
+        const float err = __fadd_rn(__fsub_rn(s, __fsub_rn(t, z)), __fsub_rn(p, z));
         s = t;
-        c += err + e;
+        c = __fadd_rn(c, __fadd_rn(err, e));
     }
     __device__ __forceinline__ void add_restart(float v, float x, bool st) {
         s = st ? 0.f : s;

@@ -134,15 +134,27 @@ extern "C" pava_status pava_spmv_csr_noalloc(int m, int n, int nnz, const int *r
                                              const double *x, double *y, void *stream) {
     (void)n;
     using namespace pava;
-    if (m < 0 || n < 0 || nnz < 0) return PAVA_E_INVALID_ARG;
+    // every error return leaves its message for pava_last_error(), as the other entry points do
+    auto fail = [](pava_status st, const std::string &msg) {
+        set_last_error("pava_spmv_csr_noalloc: " + msg);
+        return st;
+    };
+    auto fail_cuda = [&](cudaError_t err, const char *where) {
+        return fail(PAVA_E_CUDA, std::string(where) + ": " + cudaGetErrorString(err));
+    };
+    if (m < 0 || n < 0 || nnz < 0) return fail(PAVA_E_INVALID_ARG, "negative size");
     if (m == 0) return PAVA_SUCCESS;
-    if (!row_ptr || !y || (nnz > 0 && (!col_idx || !vals || !x))) return PAVA_E_INVALID_ARG;
+    if (!row_ptr || !y || (nnz > 0 && (!col_idx || !vals || !x)))
+        return fail(PAVA_E_INVALID_ARG, "NULL array");
     const long long nchunks = ((long long)nnz + NOALLOC_L - 1) / NOALLOC_L;
-    if (nchunks > NOALLOC_MAX_CHUNKS) return PAVA_E_TOO_LARGE;  // > 134,217,728 nonzeros
+    if (nchunks > NOALLOC_MAX_CHUNKS)  // > 134,217,728 nonzeros
+        return fail(PAVA_E_TOO_LARGE, "nnz " + std::to_string(nnz) +
+                                          " exceeds the 134,217,728 nonzeros its fixed scratch holds");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return PAVA_E_CUDA;
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return PAVA_E_INVALID_ARG;
+    if (e != cudaSuccess) return fail_cuda(e, "cudaGetDevice");
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return fail(PAVA_E_INVALID_ARG, "device ordinal beyond the set-up table");
     // Set-up, once per device, on the caller's current device: the device address of the
     // scratch array.  Done by the first call on that device.
     void *base = nullptr;
@@ -151,7 +163,7 @@ extern "C" pava_status pava_spmv_csr_noalloc(int m, int n, int nnz, const int *r
         if (!g_scratch_addr[dev]) {
             void *p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess || !p) return PAVA_E_CUDA;
+            if (e != cudaSuccess || !p) return fail_cuda(e, "cudaGetSymbolAddress(scratch)");
             g_scratch_addr[dev] = p;
         }
         base = g_scratch_addr[dev];
@@ -162,7 +174,7 @@ extern "C" pava_status pava_spmv_csr_noalloc(int m, int n, int nnz, const int *r
     cudaStream_t s = (cudaStream_t)stream;
     int sms = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return PAVA_E_CUDA;
+    if (e != cudaSuccess) return fail_cuda(e, "cudaDeviceGetAttribute");
     zero_empty_rows_kernel<<<(unsigned)(((long long)m + 255) / 256), 256, 0, s>>>(row_ptr, m, y);
     if (nchunks > 0) {
         long long blocks = (nchunks + NA_WARPS - 1) / NA_WARPS;
@@ -186,8 +198,8 @@ extern "C" pava_status pava_spmv_csr_noalloc(int m, int n, int nnz, const int *r
         h.meta = nullptr;
         h.carry_head = nullptr;
         h.carry_tail = nullptr;
-        if (e != cudaSuccess) return PAVA_E_CUDA;
+        if (e != cudaSuccess) return fail_cuda(e, "carry fixup launch");
     }
     e = cudaGetLastError();
-    return e == cudaSuccess ? PAVA_SUCCESS : PAVA_E_CUDA;
+    return e == cudaSuccess ? PAVA_SUCCESS : fail_cuda(e, "kernel launch");
 }

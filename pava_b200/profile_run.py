@@ -15,6 +15,11 @@ matrices, values FP32-representable; 4,096 by default).  ``--rows`` shrinks c2 /
 rows_per_tile, x_window).  ``--k K`` (CSR variants) times pava_spmm with K right-hand sides
 instead of the SpMV.  Prints one JSON line per variant with the device time of the SpMV (or
 SpMM) kernel (CUDA events) unless --quiet.
+
+``--floor`` runs the floor kernels of include/pava_probe.h on the matrix's CSR arrays instead
+(streams only, gathers at hashed columns only, column stream + gathers, values + columns +
+gathers), each over a sweep of blocks per SM, and prints the fastest launch shape of each:
+the two costs an SpMV on this matrix is made of, measured apart.
 """
 from __future__ import annotations
 
@@ -69,6 +74,8 @@ def main():
     p.add_argument("--k", type=int, default=1,
                    help="right-hand sides: k > 1 times pava_spmm on X (n x k, row-major); "
                         "CSR variants only")
+    p.add_argument("--floor", action="store_true",
+                   help="time the floor kernels (pava_probe.h) on the matrix instead")
     p.add_argument("--flush", action="store_true",
                    help="write a 512 MB buffer between timed reps (matrices smaller than L2)")
     a = p.parse_args()
@@ -82,6 +89,9 @@ def main():
     _abi.check(_abi.gpu().pava_init(0))
     A = make_matrix(a.matrix, a.rows, a.count)
     x64 = M.uniform(A.n, seed=1, fp32=True)
+    if a.floor:
+        run_floors(torch, A, x64, max(a.reps, 3), a.quiet)
+        return
     for fmt, kw in parse_variants(a.variants):
         prec = kw.get("precision", _abi.PREC_FP64)
         x = torch.from_numpy(x64).cuda()
@@ -129,6 +139,48 @@ def main():
                               "convert_ms": info["convert_ms"]}), flush=True)
         mat.close()
         del mat
+
+
+FLOOR_MODES = {0: ("streams", 12), 1: ("gathers", 0), 2: ("cols+gathers", 4),
+               3: ("vals+cols+gathers", 12)}
+
+
+def run_floors(torch, A, x_host, reps, quiet):
+    """Floor kernels over A's nonzeros in CSR order: the best of blocks per SM in {2, 4, 8, 16}
+    (256 threads) for each mode, CUDA-event timed, x resident in L2 as in an SpMV loop."""
+    from . import _abi
+    P = _abi.probe()
+    ci = torch.from_numpy(A.ci).cuda()
+    v = torch.from_numpy(A.v).cuda()
+    x = torch.from_numpy(x_host).cuda()
+    s = torch.cuda.current_stream().cuda_stream
+    for mode, (name, bpe) in FLOOR_MODES.items():
+        best = None
+        for bps in (2, 4, 8, 16):
+            out = torch.empty(P.pava_probe_floor_out_len(bps, 256), dtype=torch.float64,
+                              device="cuda")
+            args = (mode, v.data_ptr(), ci.data_ptr(), x.data_ptr(), A.nnz, A.n, 1, bps, 256,
+                    out.data_ptr(), s)
+            for _ in range(2):
+                if P.pava_probe_floor(*args) != 0:
+                    raise RuntimeError(f"pava_probe_floor mode {mode} failed")
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(reps)]
+            for e0, e1 in ev:
+                e0.record()
+                P.pava_probe_floor(*args)
+                e1.record()
+            torch.cuda.synchronize()
+            t = sorted(e0.elapsed_time(e1) for e0, e1 in ev)[len(ev) // 2]
+            if best is None or t < best[0]:
+                best = (t, bps)
+        t, bps = best
+        line = {"floor": name, "mode": mode, "matrix_nnz": A.nnz, "n": A.n, "ms": t,
+                "blocks_per_sm": bps, "threads": 256,
+                "stream_GBps": bpe * A.nnz / (t * 1e-3) / 1e9 if bpe else None,
+                "gathers_per_s": A.nnz / (t * 1e-3) if mode else None}
+        if not quiet:
+            print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

@@ -27,18 +27,21 @@ def _exported(path):
 
 
 @pytest.mark.parametrize("header,path", [("pava_gpu.h", _abi.gpu_lib_path()),
-                                         ("pava_host.h", _abi.host_lib_path())])
+                                         ("pava_host.h", _abi.host_lib_path()),
+                                         ("pava_probe.h", _abi.probe_lib_path())])
 def test_library_exports_every_declared_symbol(header, path):
     names = _declared(header)
-    assert len(names) >= 8
+    assert len(names) >= (2 if header == "pava_probe.h" else 8)
     lib = _exported(path)
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
 
 
 def test_python_bindings_cover_the_headers():
-    bound = {n for n, _, _ in _abi.GPU_SYMBOLS} | {n for n, _, _ in _abi.HOST_SYMBOLS}
-    declared = set(_declared("pava_gpu.h")) | set(_declared("pava_host.h"))
+    bound = ({n for n, _, _ in _abi.GPU_SYMBOLS} | {n for n, _, _ in _abi.HOST_SYMBOLS}
+             | {n for n, _, _ in _abi.PROBE_SYMBOLS})
+    declared = (set(_declared("pava_gpu.h")) | set(_declared("pava_host.h"))
+                | set(_declared("pava_probe.h")))
     assert declared <= bound, sorted(declared - bound)
 
 

@@ -1,5 +1,6 @@
 """pava_bench, main.cpp's CVR / CSR5 benchmark loop over the C ABI: it runs, prints the
 reference's Performance lines and passes the reference's 1 % check."""
+import json
 import os
 import re
 import subprocess
@@ -28,6 +29,14 @@ def test_driver_laplace_c1(cuda):
         assert name == "laplace_512" and int(sms) > 0 and float(conv) > 0 and float(exe) > 0
     assert "CVR status 0, rows off by more than 1%: 0" in out
     assert "CSR5 status 0, rows off by more than 1%: 0" in out
+    # one machine-readable record per section beside the Performance line
+    recs = [json.loads(l) for l in out.splitlines() if l.startswith('{"record": "pava_bench"')]
+    assert [r["section"] for r in recs] == ["CVR", "CSR5"]
+    for r in recs:
+        assert r["status"] == 0 and r["matrix"] == "laplace_512" and r["nnz"] == 1_308_672
+        assert r["GBps"] > 0 and 0 < r["roofline_frac"] < 2 and r["max_rel_err"] <= 1e-12
+        assert r["rows_off_1pct"] == 0 and r["iterations"] == 200 and r["convert_s"] > 0
+    assert recs[0]["steps"] in (32, 64, 128) and recs[1]["sigma"] == 16
 
 
 def test_driver_mtx_and_small_cvr_guard(cuda, tmp_path):

@@ -225,3 +225,26 @@ def test_config2_full_size(cuda):
         del mat
     # size-independent property: the two formats agree with each other row by row
     assert O.rel_error(ys[0], ys[1], ab, 2 * TOL)[0] == 0
+
+
+@pytest.mark.parametrize("fmt", ["cvr", "csr5", "csr"])
+def test_memory_budget_gives_nomem_and_frees(cuda, fmt):
+    """A handle whose arrays would pass the device memory budget fails with PAVA_E_NOMEM and
+    leaves no device memory behind; without the budget the same matrix converts."""
+    torch = cuda
+    L = _abi.gpu()
+    A = M.powerlaw(200_000, seed=61)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    try:
+        assert L.pava_set_device_memory_limit(1 << 20) == 0
+        with pytest.raises(_abi.PavaError) as e:
+            SpMatrix(A, fmt)
+        assert e.value.status == _abi.E_NOMEM
+    finally:
+        L.pava_set_device_memory_limit(0)
+    torch.cuda.synchronize()
+    assert abs(torch.cuda.mem_get_info()[0] - free0) < (8 << 20)
+    mat = SpMatrix(A, fmt)
+    assert mat.info()["device_bytes"] > (1 << 20)
+    mat.close()
