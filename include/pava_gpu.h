@@ -120,6 +120,19 @@ pava_status pava_init(int device);
 pava_status pava_set_device_memory_limit(unsigned long long bytes);
 unsigned long long pava_get_device_memory_limit(void);
 
+/* Bounds-checked builds (python -m pava_b200.build --bounds: libpava_gpu_bounds.so, compiled
+ * with PAVA_BOUNDS_CHECK).  Their SpMV kernels test every index that comes from data -- each
+ * x gather's column, each y row, slot numbers and tail counts read from the format's metadata,
+ * the carry chunk of a shared row -- and skip an access that would leave its array, counting
+ * it instead of faulting.  pava_bounds_checked() says whether this library is such a build;
+ * pava_bounds_report(out3, clear) synchronises the device and returns the count of failed
+ * tests, the site of the first (1 x, 2 y, 3 carry, 4 shared slot) and its index, clearing them
+ * when `clear` is set (PAVA_E_UNSUPPORTED_PARAMS in ordinary builds).  The reference has no
+ * checked build (it reads and writes its arrays unchecked); this stands in for a memory
+ * checker where none may run. */
+int pava_bounds_checked(void);
+pava_status pava_bounds_report(unsigned long long *out3, int clear);
+
 /* Converts A into `format` on the device (the GPU form of anonymouslibHandle::inputCSR +
  * asCSR5, csr5/anonymouslib_avx512.h:58-70,107-221, and of CVR's pre_processing,
  * cvr/cvr.h:583-1060).  The caller's arrays are never modified (the reference transposes

@@ -7,6 +7,8 @@
   Market reader/writer and the COO->CSR conversion (include/pava_host.h)
 * ``pava_b200/lib/pava_bench``      -- main.cpp's CVR / CSR5 benchmark loop over the C ABI
 * ``pava_b200/lib/libpava_probe.so`` -- floor kernels for measurements (include/pava_probe.h)
+* ``pava_b200/lib/libpava_gpu_bounds.so`` -- the engine built with PAVA_BOUNDS_CHECK: every
+  data-derived index tested, failures counted instead of faulting (load it with PAVA_GPU_LIB)
 
 nvcc cross-compiles for sm_100a without a GPU, so this runs on any machine with the CUDA
 toolkit.  CUDA runtime is linked statically, so the library does not depend on the
@@ -112,11 +114,20 @@ def build_probe(force: bool = False) -> str:
     return out
 
 
+def build_bounds(force: bool = False) -> str:
+    """libpava_gpu_bounds.so: the engine with PAVA_BOUNDS_CHECK, whose SpMV kernels test every
+    data-derived index and count failures instead of faulting (pava_bounds_report).  Load it
+    through PAVA_GPU_LIB, e.g. to run the GPU test suite under the checks."""
+    return build_gpu(force=force, out=os.path.join(LIBDIR, "libpava_gpu_bounds.so"),
+                     extra=("-DPAVA_BOUNDS_CHECK",))
+
+
 def build(force: bool = False) -> None:
     with ThreadPoolExecutor(max_workers=2) as ex:
         fp = ex.submit(build_probe, force)
         build_host(force)
         build_gpu(force)
+        build_bounds(force)
         fp.result()
     build_driver(force)
 

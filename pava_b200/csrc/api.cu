@@ -6,6 +6,7 @@
 
 #include <atomic>
 #include <climits>
+#include <mutex>
 #include <string>
 
 #include "pava_internal.h"
@@ -275,11 +276,62 @@ pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double 
 
 }  // namespace
 
+#ifdef PAVA_BOUNDS_CHECK
+// The bounds-check error word: [0] failed tests, [1] site of the first, [2] its index.
+__device__ unsigned long long g_guard_word[3];
+namespace {
+constexpr int GUARD_MAX_DEVICES = 64;
+void *g_guard_addr[GUARD_MAX_DEVICES] = {};
+std::mutex g_guard_mutex;
+}  // namespace
+#endif
+
 namespace pava {
 void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+unsigned long long *guard_word() {
+#ifdef PAVA_BOUNDS_CHECK
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= GUARD_MAX_DEVICES) return nullptr;
+    std::lock_guard<std::mutex> lock(g_guard_mutex);
+    if (!g_guard_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_guard_word) != cudaSuccess) return nullptr;
+        g_guard_addr[dev] = p;
+    }
+    return (unsigned long long *)g_guard_addr[dev];
+#else
+    return nullptr;
+#endif
+}
 }  // namespace pava
 
 extern "C" {
+
+int pava_bounds_checked(void) {
+#ifdef PAVA_BOUNDS_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+pava_status pava_bounds_report(unsigned long long *out3, int clear) {
+#ifdef PAVA_BOUNDS_CHECK
+    unsigned long long *w = pava::guard_word();
+    if (!w) return fail(PAVA_E_CUDA, "bounds-check error word unavailable");
+    unsigned long long h[3] = {0, 0, 0};
+    PAVA_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    PAVA_CUDA(cudaMemcpy(h, w, sizeof(h), cudaMemcpyDeviceToHost), "read bounds-check word");
+    if (clear) PAVA_CUDA(cudaMemset(w, 0, sizeof(h)), "clear bounds-check word");
+    if (out3) memcpy(out3, h, sizeof(h));
+    return PAVA_SUCCESS;
+#else
+    (void)clear;
+    if (out3) memset(out3, 0, 3 * sizeof(unsigned long long));
+    return fail(PAVA_E_UNSUPPORTED_PARAMS, "not a bounds-checked build (PAVA_BOUNDS_CHECK)");
+#endif
+}
 
 pava_status pava_set_device_memory_limit(unsigned long long bytes) {
     g_mem_limit.store(bytes);

@@ -125,7 +125,8 @@ __device__ __forceinline__ void tile_combine(double head, double tail, bool seen
                                              int next_row, int lane, int r_first, int r_last,
                                              unsigned shared, long long c, double *y,
                                              double *carry_head, double *carry_tail, int m,
-                                             int &carry_row, double &carry_val) {
+                                             int &carry_row, double &carry_val,
+                                             unsigned long long *err) {
     const unsigned sm = __ballot_sync(FULL, seen);
     const double Hs = seg_suffix(head, !seen, lane);
     double Hn = __shfl_down_sync(FULL, Hs, 1);
@@ -136,16 +137,25 @@ __device__ __forceinline__ void tile_combine(double head, double tail, bool seen
     } else {
         const int lstar = 31 - __clz(sm);
         const double own_l = tail + Hn;
-        if (seen && lane != lstar && rowcur < m) y[rowcur] = own_l;
+        if (seen && lane != lstar && rowcur < m && guard(err, rowcur >= 0, G_Y, rowcur))
+            y[rowcur] = own_l;
         const double own = __shfl_sync(FULL, own_l, lstar);
         if (carry_row >= 0 && lane == 0)
             flush_row(carry_row, carry_val + H0, r_first, r_last, shared, c, y, carry_head,
-                      carry_tail, m);
+                      carry_tail, m, err);
         carry_row = next_row;
         carry_val = own;
     }
 }
 
+// Fast paths: 1 = the bit test, park, slot step and restarts of an element share one
+// predicate (Acc<T>::step_parked); 0 = each is derived on its own
+#ifndef PAVA_F32_FUSED_STEP
+#define PAVA_F32_FUSED_STEP 1
+#endif
+#ifndef PAVA_F64_FUSED_STEP
+#define PAVA_F64_FUSED_STEP 0
+#endif
 #ifndef PAVA_CSR5_MINB32
 #define PAVA_CSR5_MINB32 3
 #endif
@@ -170,7 +180,8 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
                  const unsigned *__restrict__ desc, const VT *__restrict__ vals,
                  const IT *__restrict__ cols, const VT *__restrict__ x,
                  double *__restrict__ y, double *__restrict__ carry_head,
-                 double *__restrict__ carry_tail, long long nchunks, int G, int m) {
+                 double *__restrict__ carry_tail, long long nchunks, int G, int m, int n,
+                 unsigned long long *err) {
     constexpr int NBT = SIGMA / 4;  // blocks per tile
     // the carry fixup that follows may launch now; it waits for this grid to finish
     asm volatile("griddepcontrol.launch_dependents;");
@@ -192,7 +203,9 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
         const long long t0 = c * G;
         const VT *vb = vals + t0 * 32 * SIGMA;
         const IT *cb = cols + t0 * 32 * SIGMA;
-        const VT *xb = x + (sizeof(IT) == 2 ? (int)((unsigned)H.aux >> 1) : 0);  // offsets' base
+        const int xbase = sizeof(IT) == 2 ? (int)((unsigned)H.aux >> 1) : 0;  // offsets' base
+        const VT *xb = x + xbase;
+        const int xlo = -xbase, xhi = n - xbase;  // the offsets that stay inside x
         const int NB = G * NBT;
 
         CBlk<IT> c1 = CBlk<IT>::load(cb, 1, lane, pf);
@@ -202,7 +215,7 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
         {
             const CBlk<IT> c0 = CBlk<IT>::load(cb, 0, lane, pf);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) x0[q] = c0.gather(q, xb, pl);
+            for (int q = 0; q < 4; ++q) x0[q] = c0.gather(q, xb, pl, xlo, xhi, err);
         }
         unsigned Fn = ld_stream(desc + t0 * 32 + lane, pf);
         int rsn = tile_ptr[t0];
@@ -225,7 +238,7 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
             VT x1[4];
             if (blk + 1 < NB) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) x1[q] = c1.gather(q, xb, pl);
+                for (int q = 0; q < 4; ++q) x1[q] = c1.gather(q, xb, pl, xlo, xhi, err);
             }
             const int qb = blk % NBT;
             if (qb == 0) {  // tile start
@@ -249,6 +262,12 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
             }
             const unsigned Fb = F >> (qb * 4);
             if (fast) {  // row ends park the piece in the lane's shared slots: no branch
+#if PAVA_F64_FUSED_STEP
+                acc.template step_parked<SLOT, 1u>(Fb, sp, v0.get(0), x0[0]);
+                acc.template step_parked<SLOT, 2u>(Fb, sp, v0.get(1), x0[1]);
+                acc.template step_parked<SLOT, 4u>(Fb, sp, v0.get(2), x0[2]);
+                acc.template step_parked<SLOT, 8u>(Fb, sp, v0.get(3), x0[3]);
+#else
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const bool st = (Fb >> q) & 1u;
@@ -256,12 +275,13 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
                     sp += st ? SLOT : 0u;
                     acc.add_restart(v0.get(q), x0[q], st);
                 }
+#endif
             } else {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     if ((Fb >> q) & 1u) {
                         if (seen) {
-                            if (rowcur < m) y[rowcur] = acc.value();
+                            if (rowcur < m && guard(err, rowcur >= 0, G_Y, rowcur)) y[rowcur] = acc.value();
                         } else {
                             hpiece = acc.value();
                             seen = true;
@@ -277,7 +297,8 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
                     seen = nst > 0;
                     if (seen) hpiece = Acc<VT>::piece_at(sbase);
                     for (int k2 = 1; k2 < nst; ++k2)
-                        if (row0 + k2 < m) y[row0 + k2] = Acc<VT>::piece_at(sbase + k2 * SLOT);
+                        if (row0 + k2 < m && guard(err, row0 + k2 >= 0 && k2 < KSTK, G_Y, row0 + k2))
+                        y[row0 + k2] = Acc<VT>::piece_at(sbase + k2 * SLOT);
                     rowcur = row0 + nst;
                 }
                 if (!seen) hpiece = acc.value();
@@ -292,11 +313,12 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
                 } else {
                     const int lstar = 31 - __clz(sm);
                     const double own_l = tl + Hn;
-                    if (seen && lane != lstar && rowcur < m) y[rowcur] = own_l;
+                    if (seen && lane != lstar && rowcur < m && guard(err, rowcur >= 0, G_Y, rowcur))
+            y[rowcur] = own_l;
                     const double own = __shfl_sync(FULL, own_l, lstar);
                     if (carry_row >= 0 && lane == 0)
                         flush_row(carry_row, carry_val + H0, r_first, r_last, shared, c, y,
-                                  carry_head, carry_tail, m);
+                                  carry_head, carry_tail, m, err);
                     carry_row = rs + total - b00;
                     carry_val = own;
                 }
@@ -309,7 +331,7 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
         }
         if (carry_row >= 0 && lane == 0)
             flush_row(carry_row, carry_val, r_first, r_last, shared, c, y, carry_head,
-                      carry_tail, m);
+                      carry_tail, m, err);
     }
 }
 
@@ -326,7 +348,8 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
                      const unsigned *__restrict__ desc, const float *__restrict__ vals,
                      const IT *__restrict__ cols, const float *__restrict__ x,
                      double *__restrict__ y, double *__restrict__ carry_head,
-                     double *__restrict__ carry_tail, long long nchunks, int G, int m) {
+                     double *__restrict__ carry_tail, long long nchunks, int G, int m, int n,
+                     unsigned long long *err) {
     using VT = float;
     constexpr int NBT = SIGMA / 4;  // blocks per tile
     // the carry fixup that follows may launch now; it waits for this grid to finish
@@ -352,7 +375,9 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
         const long long t0 = c * G;
         const VT *vb = vals + t0 * 32 * SIGMA;
         const IT *cb = cols + t0 * 32 * SIGMA;
-        const VT *xb = x + (sizeof(IT) == 2 ? (int)((unsigned)H.aux >> 1) : 0);  // offsets' base
+        const int xbase = sizeof(IT) == 2 ? (int)((unsigned)H.aux >> 1) : 0;  // offsets' base
+        const VT *xb = x + xbase;
+        const int xlo = -xbase, xhi = n - xbase;  // the offsets that stay inside x
         const int NB = G * NBT;
 
         CBlk<IT> c1 = CBlk<IT>::load(cb, 1, lane, pf);
@@ -362,7 +387,7 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
         {
             const CBlk<IT> c0 = CBlk<IT>::load(cb, 0, lane, pf);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) x0[q] = c0.gather(q, xb, pl);
+            for (int q = 0; q < 4; ++q) x0[q] = c0.gather(q, xb, pl, xlo, xhi, err);
         }
         unsigned Fn = ld_stream(desc + t0 * 32 + lane, pf);
         int rsn = tile_ptr[t0];
@@ -407,9 +432,17 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
                     if ((qb + 1) / NBT == 0 || rem >= (qb + 1) / NBT) {
 #pragma unroll
                         for (int q = 0; q < 4; ++q)
-                            x1[q] = CHK ? c1.gather(q, xb, pl) : c1.gather_all(q, xb, pl);
+                            x1[q] = CHK ? c1.gather(q, xb, pl, xlo, xhi, err)
+                                        : c1.gather_all(q, xb, pl, xlo, xhi, err);
                     }
                     if (FAST) {  // row ends park the piece in the lane's shared slots
+#if PAVA_F32_FUSED_STEP
+                        const unsigned Fq = F >> (qb * 4);
+                        acc.template step_parked<SLOT, 1u>(Fq, sp, v0.get(0), x0[0]);
+                        acc.template step_parked<SLOT, 2u>(Fq, sp, v0.get(1), x0[1]);
+                        acc.template step_parked<SLOT, 4u>(Fq, sp, v0.get(2), x0[2]);
+                        acc.template step_parked<SLOT, 8u>(Fq, sp, v0.get(3), x0[3]);
+#else
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
                             const bool st = (F >> (qb * 4 + q)) & 1u;
@@ -417,12 +450,13 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
                             sp += st ? SLOT : 0u;
                             acc.add_restart(v0.get(q), x0[q], st);
                         }
+#endif
                     } else {
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
                             if ((F >> (qb * 4 + q)) & 1u) {
                                 if (seen) {
-                                    if (rowcur < m) y[rowcur] = acc.value();
+                                    if (rowcur < m && guard(err, rowcur >= 0, G_Y, rowcur)) y[rowcur] = acc.value();
                                 } else {
                                     hpiece = acc.value();
                                     seen = true;
@@ -445,7 +479,8 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
                 seen = nst > 0;
                 if (seen) hpiece = Acc<VT>::piece_at(sbase);
                 for (int k2 = 1; k2 < nst; ++k2)
-                    if (row0 + k2 < m) y[row0 + k2] = Acc<VT>::piece_at(sbase + k2 * SLOT);
+                    if (row0 + k2 < m && guard(err, row0 + k2 >= 0 && k2 < KSTK, G_Y, row0 + k2))
+                        y[row0 + k2] = Acc<VT>::piece_at(sbase + k2 * SLOT);
                 rowcur = row0 + nst;
             } else {
                 walk(Flag<false>{}, Flag<true>{});
@@ -453,11 +488,11 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
             const double a = acc.value();
             tile_combine(seen ? hpiece : a, seen ? a : 0.0, seen, rowcur, rs + total - b00,
                          lane, r_first, r_last, shared, c, y, carry_head, carry_tail, m,
-                         carry_row, carry_val);
+                         carry_row, carry_val, err);
         }
         if (carry_row >= 0 && lane == 0)
             flush_row(carry_row, carry_val, r_first, r_last, shared, c, y, carry_head,
-                      carry_tail, m);
+                      carry_tail, m, err);
     }
 }
 
@@ -481,12 +516,12 @@ void launch_sg(const Handle &h, unsigned grid, const void *x, void *y, cudaStrea
         csr5_spmv_f32_kernel<SG, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
             (const ChunkHdr *)h.meta, h.tile_ptr, h.flags, (const float *)h.vals,
             (const IT *)h.cols, (const float *)x, (double *)y, h.carry_head,
-            h.carry_tail, h.nchunks, h.G, h.m);
+            h.carry_tail, h.nchunks, h.G, h.m, h.n, guard_word());
     else
         csr5_spmv_kernel<SG, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
             (const ChunkHdr *)h.meta, h.tile_ptr, h.flags, (const VT *)h.vals,
             (const IT *)h.cols, (const VT *)x, (double *)y, h.carry_head,
-            h.carry_tail, h.nchunks, h.G, h.m);
+            h.carry_tail, h.nchunks, h.G, h.m, h.n, guard_word());
 }
 
 template <typename VT, typename IT>

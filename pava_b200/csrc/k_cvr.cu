@@ -232,7 +232,8 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
                 const VT *__restrict__ vals, const IT *__restrict__ cols,
                 const VT *__restrict__ x, const int *__restrict__ colbase,
                 double *__restrict__ y, double *__restrict__ carry_head,
-                double *__restrict__ carry_tail, long long nchunks, int m) {
+                double *__restrict__ carry_tail, long long nchunks, int m, int n,
+                unsigned long long *err) {
     constexpr int L = 32 * S;
     constexpr int NB = S / 4;
     __shared__ double s_tail[SPMV_WARPS][64];
@@ -252,7 +253,9 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
         const int i_t = M->i_t;
         const VT *vb = vals + c * L;
         const IT *cb = cols + c * L;
-        const VT *xb = x + (sizeof(IT) == 2 ? colbase[c] : 0);  // base of the column offsets
+        const int xbase = sizeof(IT) == 2 ? colbase[c] : 0;  // base of the column offsets
+        const VT *xb = x + xbase;
+        const int xlo = -xbase, xhi = n - xbase;  // the offsets that stay inside x
         const unsigned *fb = flags + c * S;
         auto LF = [&](int b) { return ld_flag(fb + ((4 * b) >> 5) * 32 + lane); };
 
@@ -270,7 +273,7 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
         {
             const CBlk<IT> c0 = CBlk<IT>::load(cb, 0, lane, pf);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) x0[q] = c0.gather(q, xb, pl);
+            for (int q = 0; q < 4; ++q) x0[q] = c0.gather(q, xb, pl, xlo, xhi, err);
         }
 #pragma unroll 1
         for (int blk = 0; blk < NB; ++blk) {
@@ -285,7 +288,7 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
             VT x1[4];
             if (blk + 1 < NB) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) x1[q] = c1.gather(q, xb, pl);
+                for (int q = 0; q < 4; ++q) x1[q] = c1.gather(q, xb, pl, xlo, xhi, err);
             }
             const unsigned fw = f0;
 #pragma unroll
@@ -297,7 +300,7 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
                     const unsigned bal = __ballot_sync(FULL, f);
                     if (f) {
                         flush_row(r_first + g, acc.value(), r_first, r_last, shared, c, y,
-                                  carry_head, carry_tail, m);
+                                  carry_head, carry_tail, m, err);
                         acc.reset();
                         g = next_g + __popc(bal & lt);
                     }
@@ -308,7 +311,7 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
                         s_tail[w][lane + 32] = 0.0;
                         __syncwarp();
                         const int pk = M->park[lane];
-                        if (pk != 0xff) {
+                        if (pk != 0xff && guard(err, pk < 64, G_SLOT, pk)) {
                             s_tail[w][pk] = acc.value();
                             s_row[w][pk] = r_first + g;
                         }
@@ -323,7 +326,8 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
                         const double a = acc.value();
                         if (i == S - 1) { last = a; last_nfrag = nfrag; }
                         else if (nfrag == 0 && cont) cin = a;
-                        else s_tail[w][slot] += a;  // a fragment that starts in this lane
+                        else if (guard(err, slot >= 0 && slot < 64, G_SLOT, slot))
+                            s_tail[w][slot] += a;  // a fragment that starts in this lane
                         ++slot;
                         ++nfrag;
                         acc.reset();
@@ -344,13 +348,18 @@ cvr_spmv_kernel(const CvrMeta *__restrict__ meta, const unsigned *__restrict__ f
             const double a = (single && cont) ? last : (cont ? cin : 0.0);
             const double H = seg_suffix(a, single && cont && link, lane);
             const double Hn = __shfl_down_sync(FULL, H, 1);
-            if (!(single && cont)) s_tail[w][slot - 1] += last + (link ? Hn : 0.0);
+            if (!(single && cont) && guard(err, slot >= 1 && slot <= 64, G_SLOT, slot - 1))
+                s_tail[w][slot - 1] += last + (link ? Hn : 0.0);
             __syncwarp();
-            const int ntail = M->ntail, n_in = M->n_inprog, ng = M->next_g;
+            int ntail = M->ntail, n_in = M->n_inprog;
+            const int ng = M->next_g;
+            if (!guard(err, ntail >= 0 && ntail <= 64 && n_in >= 0 && n_in <= ntail, G_SLOT,
+                       ntail))
+                ntail = n_in = 0;
             for (int j = lane; j < ntail; j += 32) {
                 const int row = j < n_in ? s_row[w][j] : r_first + ng + (j - n_in);
                 flush_row(row, s_tail[w][j], r_first, r_last, shared, c, y, carry_head,
-                          carry_tail, m);
+                          carry_tail, m, err);
             }
             __syncwarp();
         }
@@ -379,17 +388,17 @@ cudaError_t spmv_t(const Handle &h, const void *x, void *y, cudaStream_t s) {
         case 32:
             cvr_spmv_kernel<32, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
                 meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, h.colbase, yv,
-                h.carry_head, h.carry_tail, h.nchunks, h.m);
+                h.carry_head, h.carry_tail, h.nchunks, h.m, h.n, guard_word());
             break;
         case 64:
             cvr_spmv_kernel<64, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
                 meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, h.colbase, yv,
-                h.carry_head, h.carry_tail, h.nchunks, h.m);
+                h.carry_head, h.carry_tail, h.nchunks, h.m, h.n, guard_word());
             break;
         case 128:
             cvr_spmv_kernel<128, VT, IT><<<grid, SPMV_WARPS * 32, 0, s>>>(
                 meta, h.flags, (const VT *)h.vals, (const IT *)h.cols, xv, h.colbase, yv,
-                h.carry_head, h.carry_tail, h.nchunks, h.m);
+                h.carry_head, h.carry_tail, h.nchunks, h.m, h.n, guard_word());
             break;
         default:
             return cudaErrorInvalidValue;

@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(GROUP_THREADS, KCT ? COOP_MINB : group_minb<KP
 csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                  const VT *__restrict__ v, const VT *__restrict__ X, long long ldx,
                  double *__restrict__ Y, long long ldy, int m, int k, int gl_shift,
-                 int kc_shift, int tile_rows) {
+                 int kc_shift, int tile_rows, int n, unsigned long long *err) {
     constexpr int U = group_unroll<KPL>();
     const int lane = threadIdx.x & 31;
     const int gl = 1 << gl_shift, kc = 1 << kc_shift;
@@ -146,6 +146,7 @@ csr_group_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
     for (int p = 0; p < KPL; ++p) colok[p] = col_of<VW>(cl, p, kc) < k;
     // reads the VW columns of slot q of X row `col` and accumulates them
     auto xread = [&](int col, int q, VT val, Acc<VT>(&acc)[KPL]) {
+        if (!guard(err, col >= 0 && col < n, G_X, col)) return;
         const VT *xr = X + (long long)col * ldx + col_of<VW>(cl, q * VW, kc);
         if (VW == 2) {
             const auto x2 = ld_x2(xr, pl);
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(GROUP_THREADS, WINDOW_MINB)
 csr_window_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                   const VT *__restrict__ v, const VT *__restrict__ X, long long ldx,
                   double *__restrict__ Y, long long ldy, int m, int k, int gl_shift,
-                  int kc_shift, int tile_rows, int max_w) {
+                  int kc_shift, int tile_rows, int max_w, int n, unsigned long long *err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     VT *xs = reinterpret_cast<VT *>(smem_raw);
     constexpr int WARPS = GROUP_THREADS / 32;
@@ -265,7 +266,8 @@ csr_window_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
             cmax = s_max[q] > cmax ? s_max[q] : cmax;
         }
         const int W = cmax >= cmin ? cmax - cmin + 1 : 0;
-        const bool staged = W > 0 && W <= max_w;
+        const bool staged = W > 0 && W <= max_w &&
+                            guard(err, cmin >= 0 && cmax < n, G_X, cmin < 0 ? cmin : cmax);
         if (staged) {  // X[cmin .. cmax][0 .. k) -> xs, row stride k; SU loads in flight
             constexpr int SU = 8;
             const int total = W * k;  // <= WINDOW_SMEM / sizeof(VT)
@@ -314,7 +316,8 @@ csr_window_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                     coop_row<KPL, KCT, 1>(
                         a, b, gi, gl, es, e, kc, lane, ci, v, colok,
                         [&](int col, int p, VT val, Acc<VT>(&ac)[KPL]) {
-                            ac[p].add(val, ld_x(X + (long long)col * ldx + cl + p * kc, pl));
+                            if (guard(err, col >= 0 && col < n, G_X, col))
+                                ac[p].add(val, ld_x(X + (long long)col * ldx + cl + p * kc, pl));
                         },
                         acc, pf);
                 j = b;
@@ -345,7 +348,7 @@ csr_window_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
 #pragma unroll
                     for (int p = 0; p < KPL; ++p)
                         if (colok[p]) acc[p].add(val, xr[p * kc]);
-                } else {
+                } else if (guard(err, col >= 0 && col < n, G_X, col)) {
                     const VT *xr = X + (long long)col * ldx + cl;
 #pragma unroll
                     for (int p = 0; p < KPL; ++p)
@@ -401,7 +404,7 @@ cudaError_t launch_window(const Handle &h, const VT *x, long long ldx, double *y
         if (attr != cudaSuccess) return attr;
         csr_window_kernel<KPL, VT, KCT><<<grid, GROUP_THREADS, smem, s>>>(
             h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, ilog2(h.lanes_per_row),
-            ilog2(h.col_lanes), tr, max_w);
+            ilog2(h.col_lanes), tr, max_w, h.n, guard_word());
         return cudaGetLastError();
     });
 }
@@ -425,10 +428,12 @@ cudaError_t launch_rows(const Handle &h, const VT *x, long long ldx, double *y, 
         constexpr int VW2 = KPL >= 2 ? 2 : 1;
         if (vec2)
             csr_group_kernel<KPL, VT, KCT, VW2><<<grid, GROUP_THREADS, 0, s>>>(
-                h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, gs, ks, tr);
+                h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, gs, ks, tr, h.n,
+                guard_word());
         else
             csr_group_kernel<KPL, VT, KCT, 1><<<grid, GROUP_THREADS, 0, s>>>(
-                h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, gs, ks, tr);
+                h.rp, h.ci, (const VT *)h.v, x, ldx, y, ldy, h.m, k, gs, ks, tr, h.n,
+                guard_word());
         return cudaGetLastError();
     });
 }

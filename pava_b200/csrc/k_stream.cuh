@@ -50,15 +50,21 @@ template <> struct CBlk<int> {
     // x of element q: xb is x itself for 32-bit columns.  Column -1 (the dummy element of an
     // empty row, or chunk padding) reads nothing and gives 0, so a non-finite x never leaks
     // into an empty row.
+    // [xlo, xhi): the indices of xb that lie in x (tested in bounds-checked builds only)
     template <typename T>
-    __device__ __forceinline__ T gather(int q, const T *xb, uint64_t pol) const {
+    __device__ __forceinline__ T gather(int q, const T *xb, uint64_t pol, int xlo = 0,
+                                        int xhi = 0, unsigned long long *err = nullptr) const {
         const int c = col(q, 0);
-        return c >= 0 ? ld_x(xb + c, pol) : T(0);
+        if (c < 0 || !guard(err, c >= xlo && c < xhi, G_X, c)) return T(0);
+        return ld_x(xb + c, pol);
     }
     // the same where every element of the chunk reads x
     template <typename T>
-    __device__ __forceinline__ T gather_all(int q, const T *xb, uint64_t pol) const {
-        return ld_x(xb + col(q, 0), pol);
+    __device__ __forceinline__ T gather_all(int q, const T *xb, uint64_t pol, int xlo = 0,
+                                            int xhi = 0, unsigned long long *err = nullptr) const {
+        const int c = col(q, 0);
+        if (!guard(err, c >= xlo && c < xhi, G_X, c)) return T(0);
+        return ld_x(xb + c, pol);
     }
     int4 a;
     __device__ __forceinline__ int col(int q, int) const {
@@ -73,15 +79,19 @@ template <> struct CBlk<int> {
 template <> struct CBlk<short> {
     // x of element q: xb = x + (the chunk's base column); the offset DELTA_NONE reads nothing
     template <typename T>
-    __device__ __forceinline__ T gather(int q, const T *xb, uint64_t pol) const {
+    __device__ __forceinline__ T gather(int q, const T *xb, uint64_t pol, int xlo = 0,
+                                        int xhi = 0, unsigned long long *err = nullptr) const {
         const unsigned w = q < 2 ? a.x : a.y;
         const int d = (q & 1) ? ((int)w >> 16) : ((int)(w << 16) >> 16);
-        return d != DELTA_NONE ? ld_x(xb + d, pol) : T(0);
+        if (d == DELTA_NONE || !guard(err, d >= xlo && d < xhi, G_X, d)) return T(0);
+        return ld_x(xb + d, pol);
     }
     template <typename T>
-    __device__ __forceinline__ T gather_all(int q, const T *xb, uint64_t pol) const {
+    __device__ __forceinline__ T gather_all(int q, const T *xb, uint64_t pol, int xlo = 0,
+                                            int xhi = 0, unsigned long long *err = nullptr) const {
         const unsigned w = q < 2 ? a.x : a.y;
         const int d = (q & 1) ? ((int)w >> 16) : ((int)(w << 16) >> 16);
+        if (!guard(err, d >= xlo && d < xhi, G_X, d)) return T(0);
         return ld_x(xb + d, pol);
     }
     uint2 a;
@@ -138,6 +148,20 @@ template <> struct Acc<double> {
     }
     double s = 0.0;
     __device__ __forceinline__ void add(double v, double x) { s = fma(v, x, s); }
+    // Acc<float>::step_parked for FP64: park s at sp when the bit is set, step sp, restart.
+    template <unsigned SLOT, unsigned MASK>
+    __device__ __forceinline__ void step_parked(unsigned F, unsigned &sp, double v, double x) {
+        asm volatile(
+            "{ .reg .pred q; .reg .b32 t;\n\t"
+            "and.b32 t, %2, %3;\n\t"
+            "setp.ne.u32 q, t, 0;\n\t"
+            "@q st.shared.f64 [%0], %1;\n\t"
+            "@q add.u32 %0, %0, %4;\n\t"
+            "selp.f64 %1, 0d0000000000000000, %1, q; }"
+            : "+r"(sp), "+d"(s)
+            : "r"(F), "n"(MASK), "n"(SLOT));
+        s = fma(v, x, s);
+    }
     __device__ __forceinline__ double value() const { return s; }
     __device__ __forceinline__ void reset() { s = 0.0; }
 };
@@ -162,6 +186,24 @@ template <> struct Acc<float> {
     __device__ __forceinline__ void add_restart(float v, float x, bool st) {
         s = st ? 0.f : s;
         c = st ? 0.f : c;
+        add(v, x);
+    }
+    // One element of the branch-free row walk: when the MASK bit of the lane's row-start mask
+    // F is set, the element starts a row, so the finished piece (s, c) is parked at the shared
+    // address sp, sp moves to the lane's next slot and the sums restart; then v*x is added.
+    // The bit test, the park, the slot step and both restarts share one predicate.
+    template <unsigned SLOT, unsigned MASK>
+    __device__ __forceinline__ void step_parked(unsigned F, unsigned &sp, float v, float x) {
+        asm volatile(
+            "{ .reg .pred q; .reg .b32 t;\n\t"
+            "and.b32 t, %3, %4;\n\t"
+            "setp.ne.u32 q, t, 0;\n\t"
+            "@q st.shared.v2.f32 [%0], {%1, %2};\n\t"
+            "@q add.u32 %0, %0, %5;\n\t"
+            "selp.f32 %1, 0f00000000, %1, q;\n\t"
+            "selp.f32 %2, 0f00000000, %2, q; }"
+            : "+r"(sp), "+f"(s), "+f"(c)
+            : "r"(F), "n"(MASK), "n"(SLOT));
         add(v, x);
     }
     __device__ __forceinline__ double value() const { return (double)s + (double)c; }

@@ -51,7 +51,7 @@ __global__ void carry_fixup_kernel(const char *__restrict__ meta, size_t stride,
                                    const int *__restrict__ arp, long long L,
                                    const double *__restrict__ carry_head,
                                    const double *__restrict__ carry_tail, double *__restrict__ y,
-                                   long long nchunks, int m) {
+                                   long long nchunks, int m, unsigned long long *err) {
     // launched as a programmatic dependent of the SpMV kernel: wait until that grid has
     // finished and its carries are visible (returns at once for an ordinary launch)
     asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -64,8 +64,9 @@ __global__ void carry_fixup_kernel(const char *__restrict__ meta, size_t stride,
         if (!(sh & 1u)) continue;
         if ((sh & 2u) && H->nrows == 1) continue;  // R runs through c1 and beyond
         const int R = H->r_first;
-        if (R >= m) continue;
+        if (R >= m || !guard(err, R >= 0, G_Y, R)) continue;
         const long long c0 = (long long)arp[R] / L;
+        if (!guard(err, c0 >= 0 && c0 <= c1, G_CARRY, c0)) continue;
         double p = 0.0;
         for (long long j = c0 + 1 + lane; j <= c1; j += 32) p += carry_head[j];
         p = warp_sum(p);
@@ -173,7 +174,8 @@ cudaError_t carry_fixup(const Handle &h, void *y, cudaStream_t s) {
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, carry_fixup_kernel, (const char *)h.meta, h.meta_stride,
                               (const int *)h.arp, h.L, (const double *)h.carry_head,
-                              (const double *)h.carry_tail, (double *)y, h.nchunks, h.m);
+                              (const double *)h.carry_tail, (double *)y, h.nchunks, h.m,
+                              guard_word());
 }
 
 }  // namespace pava

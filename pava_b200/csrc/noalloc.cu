@@ -56,7 +56,7 @@ csr_tiles_noalloc_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                          const double *__restrict__ v, const double *__restrict__ x,
                          double *__restrict__ y, int m, int nnz, long long nchunks,
                          ChunkHdr *__restrict__ hdr, double *__restrict__ carry_head,
-                         double *__restrict__ carry_tail) {
+                         double *__restrict__ carry_tail, int n, unsigned long long *err) {
     const int lane = threadIdx.x & 31;
     const long long nwarps = (long long)gridDim.x * NA_WARPS;
     for (long long c = (long long)blockIdx.x * NA_WARPS + (threadIdx.x >> 5); c < nchunks;
@@ -95,7 +95,8 @@ csr_tiles_noalloc_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
                 } else if (el == e0 && (long long)rp[row] == el) {
                     seen = true;  // the lane's first element starts its row
                 }
-                acc = fma(v[el], x[ci[el]], acc);
+                const int col = ci[el];
+                if (guard(err, col >= 0 && col < n, G_X, col)) acc = fma(v[el], x[col], acc);
             }
             if (!seen) hpiece = acc;
             const double tl = seen ? acc : 0.0;
@@ -132,7 +133,6 @@ csr_tiles_noalloc_kernel(const int *__restrict__ rp, const int *__restrict__ ci,
 extern "C" pava_status pava_spmv_csr_noalloc(int m, int n, int nnz, const int *row_ptr,
                                              const int *col_idx, const double *vals,
                                              const double *x, double *y, void *stream) {
-    (void)n;
     using namespace pava;
     // every error return leaves its message for pava_last_error(), as the other entry points do
     auto fail = [](pava_status st, const std::string &msg) {
@@ -180,7 +180,7 @@ extern "C" pava_status pava_spmv_csr_noalloc(int m, int n, int nnz, const int *r
         long long blocks = (nchunks + NA_WARPS - 1) / NA_WARPS;
         if (blocks > (long long)sms * 8) blocks = (long long)sms * 8;
         csr_tiles_noalloc_kernel<<<(unsigned)blocks, NA_WARPS * 32, 0, s>>>(
-            row_ptr, col_idx, vals, x, y, m, nnz, nchunks, hdr, head, tail);
+            row_ptr, col_idx, vals, x, y, m, nnz, nchunks, hdr, head, tail, n, guard_word());
         // the unchanged carry fixup, pointed at the scratch: chunk c's first element is
         // c*L and a shared row R starts in chunk row_ptr[R] / L
         Handle h;

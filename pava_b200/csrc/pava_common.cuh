@@ -112,6 +112,37 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane) {
     return s - v;
 }
 
+// ---- bounds-checked builds ---------------------------------------------------------------
+// Built with -DPAVA_BOUNDS_CHECK (python -m pava_b200.build --bounds), the SpMV kernels test
+// every index that comes from data before they use it -- the column of each x gather, the row
+// of each y store, slot numbers read from the format's metadata, the carry chunk of a shared
+// row.  A failed test increments the error word err[0] (the first failure also leaves its site
+// in err[1] and the index in err[2]) and the access is skipped, so a bad index becomes a
+// status the host reads (pava_bounds_report) instead of a fault.  In ordinary builds the tests
+// compile to nothing.
+enum GuardSite : unsigned {
+    G_X = 1,      // x gather column outside [0, n)
+    G_Y = 2,      // y row outside [0, m)
+    G_CARRY = 3,  // carry chunk outside [0, nchunks)
+    G_SLOT = 4,   // shared-memory slot or tail count from the metadata outside its array
+};
+
+__device__ __forceinline__ bool guard(unsigned long long *err, bool ok, unsigned site,
+                                      long long idx) {
+#ifdef PAVA_BOUNDS_CHECK
+    if (!ok && err) {
+        if (atomicAdd(err, 1ull) == 0ull) {
+            err[1] = site;
+            err[2] = (unsigned long long)idx;
+        }
+    }
+    return ok;
+#else
+    (void)err; (void)ok; (void)site; (void)idx;
+    return true;
+#endif
+}
+
 // Common prefix of every chunk's metadata: rows the chunk touches and whether its first /
 // last row continues into the neighbouring chunk.  The carry fixup reads only this prefix.
 struct ChunkHdr {
@@ -127,10 +158,11 @@ struct ChunkHdr {
 template <typename YT>
 __device__ __forceinline__ void flush_row(int row, double val, int r_first, int r_last,
                                           unsigned shared, long long c, YT *y,
-                                          double *carry_head, double *carry_tail, int m) {
+                                          double *carry_head, double *carry_tail, int m,
+                                          unsigned long long *err = nullptr) {
     if (row == r_first && (shared & 1u)) carry_head[c] = val;
     else if (row == r_last && (shared & 2u)) carry_tail[c] = val;
-    else if (row < m) y[row] = (YT)val;
+    else if (row < m && guard(err, row >= 0, G_Y, row)) y[row] = (YT)val;
 }
 
 }  // namespace pava

@@ -67,6 +67,10 @@ struct Handle {
 // Sets the message pava_last_error() returns on this thread.
 void set_last_error(const std::string &msg);
 
+// Device address of the bounds-check error word (three 64-bit words) on the current device in
+// builds with PAVA_BOUNDS_CHECK; nullptr in ordinary builds, whose kernels never test it.
+unsigned long long *guard_word();
+
 // CSR5 tiles per chunk.  The persistent grid keeps `warps` warps resident (24 per SM); each
 // takes chunks in turn, so a chunk count just above a multiple of `warps` leaves a last wave
 // that few warps run.

@@ -23,6 +23,24 @@ def _ensure_built():
 _ensure_built()
 
 
+@pytest.fixture(autouse=True)
+def _bounds_report(request):
+    """With a bounds-checked engine loaded (PAVA_GPU_LIB=.../libpava_gpu_bounds.so), every GPU
+    test must leave the error word at zero: no kernel met an index outside its arrays."""
+    yield
+    if "cuda" not in request.fixturenames:
+        return
+    import ctypes
+    from pava_b200 import _abi
+    L = _abi.gpu()
+    if not L.pava_bounds_checked():
+        return
+    out = (ctypes.c_ulonglong * 3)()
+    _abi.check(L.pava_bounds_report(out, 1))
+    assert out[0] == 0, (f"bounds check: {out[0]} failed index tests, the first at site "
+                         f"{out[1]} with index {out[2]}")
+
+
 @pytest.fixture(scope="session")
 def cuda():
     import torch
