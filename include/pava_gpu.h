@@ -76,7 +76,9 @@ typedef struct pava_opts {
                              matrix gives fewer than 24 chunks of 64 steps per SM) */
     int sigma;            /* CSR5: elements per lane per tile, 8, 12, 16, 24 or 32 (default 16) */
     int tiles_per_chunk;  /* CSR5: tiles per warp chunk, 1 .. 64 (default 4; 2 or 1 when a
-                             matrix gives fewer than 4 x 24 tiles per SM) */
+                             matrix gives fewer than 4 x 24 tiles per SM), or PAVA_TILES_WAVE
+                             (-1): the count in 1 .. 8 that fills the last wave of resident
+                             warps best for this matrix */
     int precision;        /* pava_precision */
     int index_mode;       /* pava_index_mode */
     int lanes_per_row;    /* CSR: lanes per row group, 1, 2, 4, 8, 16 or 32 (default: from
@@ -293,22 +295,35 @@ pava_status pava_gen_device(const pava_gen_params *p, uint64_t seed, void *strea
 pava_status pava_free_device_csr(pava_csr *A);
 
 /* ---- Learned form selector ----------------------------------------------------------
- * No counterpart in the reference (which runs every format it is asked for).  Six engine
- * variants -- the form and its tile parameter:
- *   0 CVR steps 64    1 CVR steps 128    2 CSR5 sigma 16    3 CSR5 sigma 32
- *   4 CSR 4 lanes per row                5 CSR 32 lanes per row
- * A matrix is described by 12 structural features (pava_features), an MLP 12-64-64-6
- * predicts the log-time of each variant, and the smallest prediction wins.  The network is
- * trained on the GPU by the library's own forward / backward / Adam kernels on timings that
- * pava_time_variants measures; exhaustive timing is both the fallback and the yardstick of
- * the selector's regret. */
-#define PAVA_NVARIANTS 6
+ * No counterpart in the reference (which runs every format it is asked for; its only tile
+ * knob is CSR5's sigma, anonymouslibHandle::setSigma, csr5/anonymouslib_avx512.h:265).
+ * The selector chooses among PAVA_NVARIANTS = 30 engine forms: a kernel variant and its tile
+ * parameters, the same set pava_autotune searches for one right-hand side:
+ *    0 ..  3  CVR, steps 64 / 128, each with 32-bit columns and with PAVA_INDEX_AUTO
+ *             (v = 2 * (steps == 128) + auto)
+ *    4 .. 11  CSR5, sigma 16 / 32, default tiles per chunk or the wave-balanced count
+ *             (PAVA_TILES_WAVE), 32-bit columns or PAVA_INDEX_AUTO
+ *             (v = 4 + 4 * (sigma == 32) + 2 * wave + auto)
+ *   12 .. 29  plain CSR row groups, lanes per row 1, 2, 4, 8, 16, 32, with 1, 4 or 16 row
+ *             groups per warp tile (v = 12 + 3 * log2(lanes) + {0, 1, 2})
+ * Forms fall into PAVA_NFAMILIES = 6 kernel variants (pava_variant_family): CVR 64, CVR 128,
+ * CSR5 16, CSR5 32, CSR with <= 4 lanes per row, CSR with >= 8.  A matrix is described by 12
+ * structural features (pava_features); an MLP 12-64-64-30 predicts the log-time of every form
+ * (so also each variant's best time, the minimum over its forms) and the smallest prediction
+ * wins.  The network is trained on the GPU by the library's own forward / backward / Adam
+ * kernels on timings that pava_time_variants measures; exhaustive timing of all 30 forms is
+ * both the fallback and the yardstick of the selector's regret. */
+#define PAVA_NVARIANTS 30
+#define PAVA_NFAMILIES 6
+#define PAVA_TILES_WAVE (-1) /* pava_opts.tiles_per_chunk: the wave-balanced count for A */
 #define PAVA_MLP_IN 12
 #define PAVA_MLP_HIDDEN 64
-#define PAVA_MLP_OUT 6
-#define PAVA_MLP_NPARAM 5382
-/* Variant v's format and options (options zeroed except the variant's tile parameter). */
+#define PAVA_MLP_OUT 30
+#define PAVA_MLP_NPARAM 6942
+/* Form v's format and options (options zeroed except the form's tile parameters). */
 pava_status pava_variant(int v, int *format, pava_opts *opts);
+/* The kernel variant (0 .. PAVA_NFAMILIES - 1) form v belongs to, or -1 if v is out of range. */
+int pava_variant_family(int v);
 /* Structural features of a device CSR (sorted columns), 12 floats:
  *   0 log10 m   1 log10 nnz   2 log10 mean row length   3 row-length std / mean
  *   4 log10 max / mean row length   5 share of empty rows   6 share of nonzeros in rows
@@ -316,23 +331,25 @@ pava_status pava_variant(int v, int *format, pava_opts *opts);
  *   9 share of nonzeros within 64 of the diagonal   10 distinct 128-byte x lines per
  *   nonzero   11 log10(mean row span / n + 1e-7).  Integer accumulation: same bits each run. */
 pava_status pava_features(const pava_csr *A, float *out12, void *stream);
-/* Converts A into each variant and times its SpMV (one warm-up, median of `reps` CUDA-event
- * timings, x and y on the device); ms[v] < 0 when variant v failed; *best = fastest. */
+/* Converts A into each of the 30 forms and times its SpMV (two warm-ups, median of `reps`
+ * CUDA-event timings, x and y on the device): pava_autotune for k = 1, in form order.
+ * ms[v] < 0 when form v failed; a wave-balanced CSR5 form whose tile count equals the default
+ * one is the same form and gets its twin's time; *best = fastest. */
 pava_status pava_time_variants(const pava_csr *A, int reps, double *ms, int *best);
 typedef struct pava_mlp pava_mlp;
 /* A network with He-uniform weights from `seed`, zero biases, identity normalisation. */
 pava_status pava_mlp_create(uint64_t seed, pava_mlp **out);
-/* Parameters (PAVA_MLP_NPARAM floats: W1[64][12] b1 W2[64][64] b2 W3[6][64] b3) and the
+/* Parameters (PAVA_MLP_NPARAM floats: W1[64][12] b1 W2[64][64] b2 W3[30][64] b3) and the
  * feature normalisation (x - mean) / std applied to every batch; any pointer may be NULL.
  * Setting parameters resets the Adam state. */
 pava_status pava_mlp_get_params(const pava_mlp *m, float *params, float *mean12, float *std12);
 pava_status pava_mlp_set_params(pava_mlp *m, const float *params, const float *mean12,
                                 const float *std12);
-/* Uploads a batch: B x 12 raw features, optional B x 6 targets and 0/1 mask (NULL mask = all
+/* Uploads a batch: B x 12 raw features, optional B x 30 targets and 0/1 mask (NULL mask = all
  * ones).  The loss is the masked mean squared error. */
 pava_status pava_mlp_set_batch(pava_mlp *m, int B, const float *X, const float *T,
                                const float *mask);
-/* Outputs for the current batch (B x 6, host). */
+/* Outputs for the current batch (B x 30, host). */
 pava_status pava_mlp_forward(pava_mlp *m, float *Y);
 /* Gradient of the loss w.r.t. the parameters (PAVA_MLP_NPARAM floats, host) and the loss. */
 pava_status pava_mlp_gradient(pava_mlp *m, float *grad, float *loss);
@@ -340,11 +357,11 @@ pava_status pava_mlp_gradient(pava_mlp *m, float *grad, float *loss);
  * loss_hist (may be NULL) receives the loss before each step. */
 pava_status pava_mlp_train(pava_mlp *m, int epochs, float lr, float *loss_hist);
 pava_status pava_mlp_destroy(pava_mlp *m);
-/* The variant the network predicts fastest for a device CSR (and the 6 predictions).  Uses
+/* The form the network predicts fastest for a device CSR (and the 30 predictions).  Uses
  * the network's batch slot (a 1-sample batch replaces the current one). */
-pava_status pava_select(pava_mlp *m, const pava_csr *A, int *variant, float *pred6);
-/* pava_create with the selected variant: by the network when m != NULL and A is on the
- * device, otherwise by timing all six (the exhaustive fallback). */
+pava_status pava_select(pava_mlp *m, const pava_csr *A, int *variant, float *pred30);
+/* pava_create with the selected form: by the network when m != NULL and A is on the
+ * device, otherwise by timing all 30 (the exhaustive fallback). */
 pava_status pava_create_selected(const pava_csr *A, pava_mlp *m, void *stream,
                                  pava_handle **out, int *variant);
 

@@ -75,7 +75,8 @@ class PavaGenParams(ctypes.Structure):
 
 
 GEN_STENCIL, GEN_BANDED, GEN_POWERLAW, GEN_BLOCKDIAG = 0, 1, 2, 3
-NVARIANTS, MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_NPARAM = 6, 12, 64, 6, 5382
+NVARIANTS, NFAMILIES, MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_NPARAM = 30, 6, 12, 64, 30, 6942
+TILES_WAVE = -1
 
 
 class PavaError(RuntimeError):
@@ -127,6 +128,7 @@ GPU_SYMBOLS = [
     ("pava_free_device_csr", c_int, [ctypes.POINTER(PavaCsr)]),
     ("pava_features", c_int, [ctypes.POINTER(PavaCsr), c_void_p, c_void_p]),
     ("pava_variant", c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(PavaOpts)]),
+    ("pava_variant_family", c_int, [c_int]),
     ("pava_time_variants", c_int, [ctypes.POINTER(PavaCsr), c_int, c_void_p,
                                    ctypes.POINTER(c_int)]),
     ("pava_mlp_create", c_int, [c_u64, ctypes.POINTER(c_void_p)]),

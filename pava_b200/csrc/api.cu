@@ -429,7 +429,9 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
         h.L = 32LL * h.S;
     } else if (format == PAVA_FORMAT_CSR5) {
         h.sigma = o.sigma ? o.sigma : 16;
-        if (o.tiles_per_chunk) {
+        if (o.tiles_per_chunk == PAVA_TILES_WAVE) {  // fill the last wave of warps best
+            h.G = pava::csr5_wave_tiles((long long)h.nnz / (32LL * h.sigma), want_chunks);
+        } else if (o.tiles_per_chunk) {
             h.G = o.tiles_per_chunk;
         } else {  // 4 tiles per chunk, fewer for small matrices
             h.G = pava::csr5_default_tiles((long long)h.nnz / (32LL * h.sigma), want_chunks);

@@ -173,10 +173,9 @@ pava_status build_union(int count, const pava_csr *mats, cudaStream_t s, pava_ba
     return PAVA_SUCCESS;
 }
 
-// Built-in candidate forms for k right-hand sides (at most 72 for any k <= 128; 30 for k = 1).
-// nnz and sm_count size the CSR5 chunks.
-std::vector<std::pair<int, pava_opts>> candidates(int k, int precision, long long nnz,
-                                                  int sm_count) {
+// Built-in candidate forms for k right-hand sides: for k = 1 the 30 forms of pava_variant in
+// their order (the selector's space); for k > 1 the row-group shapes (at most 72 for k <= 128).
+std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
     std::vector<std::pair<int, pava_opts>> c;
     auto base = [&]() {
         pava_opts o;
@@ -184,27 +183,15 @@ std::vector<std::pair<int, pava_opts>> candidates(int k, int precision, long lon
         o.precision = precision;
         return o;
     };
-    if (k == 1) {  // each with 32-bit columns and with 16-bit offsets where they reach
-        for (int im : {(int)PAVA_INDEX_I32, (int)PAVA_INDEX_AUTO}) {
-            for (int S : {64, 128}) {
-                pava_opts o = base();
-                o.steps = S;
-                o.index_mode = im;
-                c.push_back({PAVA_FORMAT_CVR, o});
-            }
-            for (int sg : {16, 32}) {  // default tiles per chunk, and wave-balanced
-                pava_opts o = base();
-                o.sigma = sg;
-                o.index_mode = im;
-                c.push_back({PAVA_FORMAT_CSR5, o});
-                const long long tiles = nnz / (32LL * sg), warps = 24LL * sm_count;
-                const int gw = pava::csr5_wave_tiles(tiles, warps);
-                if (gw != pava::csr5_default_tiles(tiles, warps)) {
-                    o.tiles_per_chunk = gw;
-                    c.push_back({PAVA_FORMAT_CSR5, o});
-                }
-            }
+    if (k == 1) {
+        for (int v = 0; v < PAVA_NVARIANTS; ++v) {
+            int f = 0;
+            pava_opts o;
+            pava_variant(v, &f, &o);
+            o.precision = precision;
+            c.push_back({f, o});
         }
+        return c;
     }
     const int kpls[3] = {1, 2, 4};
     for (int kpl : kpls) {
@@ -253,7 +240,14 @@ pava_status pava_autotune(const pava_csr *A, int k, int precision, int reps,
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return bfail(PAVA_E_CUDA, "no usable CUDA device");
-    const std::vector<std::pair<int, pava_opts>> cand = candidates(k, precision, A->nnz, sms);
+    const std::vector<std::pair<int, pava_opts>> cand = candidates(k, precision);
+    // CSR5 forms whose wave-balanced tile count equals the default count are the same form:
+    // timed once, the twin copies the result
+    auto csr5_tiles = [&](const pava_opts &o) {
+        const long long tiles = (long long)A->nnz / (32LL * o.sigma), warps = 24LL * sms;
+        if (o.tiles_per_chunk == PAVA_TILES_WAVE) return pava::csr5_wave_tiles(tiles, warps);
+        return o.tiles_per_chunk ? o.tiles_per_chunk : pava::csr5_default_tiles(tiles, warps);
+    };
     const size_t sx = precision == PAVA_PREC_FP32C ? 4 : 8;
     void *X = nullptr, *Y = nullptr;
     cudaError_t e = cudaMalloc(&X, sx * (size_t)(A->n ? A->n : 1) * k);
@@ -274,6 +268,17 @@ pava_status pava_autotune(const pava_csr *A, int k, int precision, int reps,
         t.format = cand[ci].first;
         t.opts = cand[ci].second;
         t.ms = -1.0;
+        if (t.format == PAVA_FORMAT_CSR5 && t.opts.tiles_per_chunk == PAVA_TILES_WAVE && n >= 3) {
+            // forms 4 + 4s + 2w + a: the default-tiles twin of a wave form is two entries back
+            const pava_tune_entry &tw = entries[n - 3];
+            if (tw.format == PAVA_FORMAT_CSR5 && tw.opts.tiles_per_chunk == 0 &&
+                tw.opts.sigma == t.opts.sigma && tw.opts.index_mode == t.opts.index_mode &&
+                csr5_tiles(tw.opts) == csr5_tiles(t.opts)) {
+                t.ms = tw.ms;
+                t.status = tw.status;
+                continue;
+            }
+        }
         pava_handle *H = nullptr;
         t.status = pava_create(A, t.format, &t.opts, nullptr, &H);
         if (t.status != PAVA_SUCCESS) continue;

@@ -1,6 +1,7 @@
-// The six engine variants the learned selector chooses between, their exhaustive timing, and
-// selection: features (k_features.cu) -> MLP (k_mlp.cu) -> the variant with the smallest
-// predicted log-time.  With no trained network, selection falls back to timing all six.
+// The 30 engine forms the learned selector chooses between (a kernel variant and its tile
+// parameters: the k = 1 candidate set of pava_autotune), their exhaustive timing, and
+// selection: features (k_features.cu) -> MLP (k_mlp.cu) -> the form with the smallest
+// predicted log-time.  With no trained network, selection falls back to timing all 30.
 
 #include <string.h>
 
@@ -13,81 +14,59 @@ namespace {
 
 using namespace pava;
 
-struct Variant {
-    int format;
-    int steps, sigma, lanes_per_row;
-};
-
-constexpr Variant VARIANTS[PAVA_NVARIANTS] = {
-    {PAVA_FORMAT_CVR, 64, 0, 0},  {PAVA_FORMAT_CVR, 128, 0, 0},
-    {PAVA_FORMAT_CSR5, 0, 16, 0}, {PAVA_FORMAT_CSR5, 0, 32, 0},
-    {PAVA_FORMAT_CSR, 0, 0, 4},   {PAVA_FORMAT_CSR, 0, 0, 32},
-};
+// Form v's format and options (the enumeration documented in pava_gpu.h).
+bool form_of(int v, int &format, pava_opts &o) {
+    memset(&o, 0, sizeof(o));
+    if (v < 0 || v >= PAVA_NVARIANTS) return false;
+    if (v < 4) {
+        format = PAVA_FORMAT_CVR;
+        o.steps = (v & 2) ? 128 : 64;
+        o.index_mode = (v & 1) ? PAVA_INDEX_AUTO : PAVA_INDEX_I32;
+    } else if (v < 12) {
+        const int q = v - 4;
+        format = PAVA_FORMAT_CSR5;
+        o.sigma = (q & 4) ? 32 : 16;
+        o.tiles_per_chunk = (q & 2) ? PAVA_TILES_WAVE : 0;
+        o.index_mode = (q & 1) ? PAVA_INDEX_AUTO : PAVA_INDEX_I32;
+    } else {
+        const int q = v - 12;
+        static const int groups[3] = {1, 4, 16};
+        format = PAVA_FORMAT_CSR;
+        o.lanes_per_row = 1 << (q / 3);
+        o.rows_per_tile = groups[q % 3] * (32 / o.lanes_per_row);
+    }
+    return true;
+}
 
 }  // namespace
 
 extern "C" {
 
 pava_status pava_variant(int v, int *format, pava_opts *opts) {
-    if (v < 0 || v >= PAVA_NVARIANTS) { set_last_error("variant out of range"); return PAVA_E_INVALID_ARG; }
-    if (format) *format = VARIANTS[v].format;
-    if (opts) {
-        memset(opts, 0, sizeof(*opts));
-        opts->steps = VARIANTS[v].steps;
-        opts->sigma = VARIANTS[v].sigma;
-        opts->lanes_per_row = VARIANTS[v].lanes_per_row;
-    }
+    int f = 0;
+    pava_opts o;
+    if (!form_of(v, f, o)) { set_last_error("variant out of range"); return PAVA_E_INVALID_ARG; }
+    if (format) *format = f;
+    if (opts) *opts = o;
     return PAVA_SUCCESS;
+}
+
+int pava_variant_family(int v) {
+    if (v < 0 || v >= PAVA_NVARIANTS) return -1;
+    if (v < 4) return v < 2 ? 0 : 1;
+    if (v < 12) return v < 8 ? 2 : 3;
+    return (v - 12) / 3 <= 2 ? 4 : 5;  // lanes per row <= 4 / >= 8
 }
 
 pava_status pava_time_variants(const pava_csr *A, int reps, double *ms, int *best) {
     if (!A || !ms) { set_last_error("NULL argument"); return PAVA_E_INVALID_ARG; }
-    if (reps < 1) reps = 1;
-    void *x = nullptr, *y = nullptr;
-    cudaError_t e = cudaMalloc(&x, sizeof(double) * (size_t)(A->n ? A->n : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&y, sizeof(double) * (size_t)(A->m ? A->m : 1));
-    if (e == cudaSuccess) e = cudaMemset(x, 0, sizeof(double) * (size_t)(A->n ? A->n : 1));
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (e == cudaSuccess) e = cudaEventCreate(&e0);
-    if (e == cudaSuccess) e = cudaEventCreate(&e1);
-    if (e != cudaSuccess) {
-        cudaFree(x); cudaFree(y);
-        if (e0) cudaEventDestroy(e0);
-        set_last_error(std::string("time variants: ") + cudaGetErrorString(e));
-        return PAVA_E_CUDA;
-    }
-    int bi = -1;
-    for (int v = 0; v < PAVA_NVARIANTS; ++v) {
-        ms[v] = -1.0;
-        int fmt;
-        pava_opts o;
-        pava_variant(v, &fmt, &o);
-        pava_handle *H = nullptr;
-        if (pava_create(A, fmt, &o, nullptr, &H) != PAVA_SUCCESS) continue;
-        pava_status st = pava_spmv(H, x, y, nullptr);
-        std::vector<float> t;
-        for (int r = 0; r < reps && st == PAVA_SUCCESS; ++r) {
-            cudaEventRecord(e0, nullptr);
-            st = pava_spmv(H, x, y, nullptr);
-            cudaEventRecord(e1, nullptr);
-            cudaEventSynchronize(e1);
-            float f = 0.f;
-            cudaEventElapsedTime(&f, e0, e1);
-            t.push_back(f);
-        }
-        pava_destroy(H);
-        if (st != PAVA_SUCCESS || t.empty()) continue;
-        std::sort(t.begin(), t.end());
-        ms[v] = t[t.size() / 2];
-        if (bi < 0 || ms[v] < ms[bi]) bi = v;
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaFree(x);
-    cudaFree(y);
+    std::vector<pava_tune_entry> ent(PAVA_NVARIANTS);
+    int n = 0, bi = -1;
+    const pava_status st =
+        pava_autotune(A, 1, PAVA_PREC_FP64, reps, ent.data(), PAVA_NVARIANTS, &n, &bi);
+    for (int v = 0; v < PAVA_NVARIANTS; ++v) ms[v] = v < n ? ent[v].ms : -1.0;
     if (best) *best = bi;
-    if (bi < 0) { set_last_error("no variant ran"); return PAVA_E_UNSUPPORTED_PARAMS; }
-    return PAVA_SUCCESS;
+    return st;
 }
 
 pava_status pava_select(pava_mlp *m, const pava_csr *A, int *variant, float *pred) {
@@ -96,6 +75,7 @@ pava_status pava_select(pava_mlp *m, const pava_csr *A, int *variant, float *pre
     pava_status st = pava_features(A, f, nullptr);
     if (st != PAVA_SUCCESS) return st;
     st = pava_mlp_set_batch(m, 1, f, nullptr, nullptr);
+    static_assert(PAVA_MLP_OUT == PAVA_NVARIANTS, "one network output per form");
     float o[PAVA_MLP_OUT];
     if (st == PAVA_SUCCESS) st = pava_mlp_forward(m, o);
     if (st != PAVA_SUCCESS) return st;
@@ -115,7 +95,7 @@ pava_status pava_create_selected(const pava_csr *A, pava_mlp *m, void *stream,
     pava_status st;
     if (m && A->on_device) {
         st = pava_select(m, A, &v, nullptr);
-    } else {  // no network (or a host CSR): exhaustive timing of the six variants
+    } else {  // no network (or a host CSR): exhaustive timing of the 30 forms
         double ms[PAVA_NVARIANTS];
         st = pava_time_variants(A, 3, ms, &v);
     }

@@ -9,14 +9,16 @@ lognormal power-law and block-diagonal (dense blocks of 8..64); rows log-uniform
 [10^4, 10^7] and nonzeros log-uniform in [10^5, 10^8] (each family's row length follows
 from the pair, within its own range); values N(0,1), FP64.  Every matrix is generated on the
 GPU (pava_gen_device), described by its 12 structural features (pava_features), and each of
-the six engine variants is converted and timed on it (pava_time_variants: median of 5
-CUDA-event timings after a warm-up, x and y resident).  The file keeps the features, the
+the 30 engine forms -- six kernel variants with their tile parameters, the k = 1 candidate
+set of pava_autotune -- is converted and timed on it (pava_time_variants: median of 5
+CUDA-event timings after two warm-ups, x and y resident).  The file keeps the features, the
 times and each matrix's family, rows and nonzeros.
 
-Network: MLP 12-64-64-6 (ReLU, FP32), trained on the GPU by the library's own kernels
+Network: MLP 12-64-64-30 (ReLU, FP32), trained on the GPU by the library's own kernels
 (pava_mlp_train: full-batch Adam on the masked mean squared error of standardised
-log-times).  Selection = the variant with the smallest predicted log-time.  Regret of a
-choice = t_chosen / t_best - 1, t_best from the exhaustive timing of all six variants.
+log-times).  Selection = the form with the smallest predicted log-time; a kernel variant's
+predicted time is the smallest over its forms.  Regret of a choice = t_chosen / t_best - 1,
+t_best from the exhaustive timing of all 30 forms (the full autotune).
 """
 from __future__ import annotations
 
@@ -30,7 +32,30 @@ import numpy as np
 from . import _abi
 
 FAMILIES = ["stencil", "banded", "powerlaw", "blockdiag"]
-VARIANT_NAMES = ["cvr_s64", "cvr_s128", "csr5_s16", "csr5_s32", "csr_l4", "csr_l32"]
+FAMILY_NAMES = ["cvr_s64", "cvr_s128", "csr5_s16", "csr5_s32", "csr_l1_4", "csr_l8_32"]
+
+
+def _form_names():
+    out = []
+    for s_ in (64, 128):
+        for a in ("i32", "auto"):
+            out.append(f"cvr_s{s_}_{a}")
+    for sg in (16, 32):
+        for w in ("tiles_default", "tiles_wave"):
+            for a in ("i32", "auto"):
+                out.append(f"csr5_s{sg}_{w}_{a}")
+    for gl in (1, 2, 4, 8, 16, 32):
+        for g in (1, 4, 16):
+            out.append(f"csr_l{gl}_g{g}")
+    return out
+
+
+FORM_NAMES = _form_names()
+# the kernel variant each form belongs to (pava_variant_family)
+FORM_FAMILY = np.array([0, 0, 1, 1] + [2] * 4 + [3] * 4 + [4] * 9 + [5] * 9)
+# each variant's default form, the one a selector of the kernel variant alone would run (CVR /
+# CSR5 with default tiles and 32-bit columns, CSR 4 and 32 lanes with 4 row groups per tile)
+FAMILY_DEFAULT_FORM = np.array([0, 2, 4, 8, 12 + 3 * 2 + 1, 12 + 3 * 5 + 1])
 N_TRAIN, N_TEST = 2000, 200
 
 
@@ -236,6 +261,11 @@ def train_selector(data, epochs=3000, lr=3e-3, seed=0):
     tr_reg = np.stack([regret(Tms[:ntr], np.full(ntr, v)) for v in range(_abi.NVARIANTS)])
     fixed = int(np.argmin(np.where(np.isfinite(tr_reg), tr_reg, 1e9).mean(1)))
     reg_fixed = regret(Tms[ntr:], np.full(len(Fte), fixed))
+    # the network asked only for the kernel variant, each variant run with its default tile
+    # parameters: what predicting the tile parameters adds
+    fam_pred = np.stack([np.where(FORM_FAMILY == f, pred, np.inf).min(1)
+                         for f in range(_abi.NFAMILIES)], 1)
+    reg_family = regret(Tms[ntr:], FAMILY_DEFAULT_FORM[fam_pred.argmin(1)])
     report = {
         "train_loss_first": float(hist[0]), "train_loss_last": float(hist[-1]),
         "train_regret_mean": float(regret(Tms[:ntr], pred_tr.argmin(1)).mean()),
@@ -244,8 +274,9 @@ def train_selector(data, epochs=3000, lr=3e-3, seed=0):
         "selector_regret_median": float(np.median(reg)),
         "selector_regret_p90": float(np.quantile(reg, 0.9)),
         "selector_top1": float((reg == 0).mean()),
-        "fixed_variant": VARIANT_NAMES[fixed],
+        "fixed_form": FORM_NAMES[fixed],
         "fixed_regret_mean": float(reg_fixed.mean()),
+        "variant_only_regret_mean": float(reg_family.mean()),
         "oracle_best_counts": np.bincount(np.argmin(np.where(Tms[ntr:] > 0, Tms[ntr:], np.inf), 1),
                                           minlength=_abi.NVARIANTS).tolist(),
         "selector_choice_counts": np.bincount(choice, minlength=_abi.NVARIANTS).tolist(),

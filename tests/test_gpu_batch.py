@@ -252,9 +252,10 @@ def test_autotune_k1_runs_every_candidate(cuda):
 
 
 def test_autotune_wave_balanced_csr5(cuda):
-    """CSR5 candidates also come with the tiles per chunk that fill the last wave of warp
-    chunks (24 resident warps per SM): on the 1,048,576-row banded matrix, sigma 32 has
-    24,576 tiles; 7 per chunk make 3,511 chunks, one wave on 148 SMs."""
+    """CSR5 candidates come with the default tiles per chunk and with PAVA_TILES_WAVE, the
+    count that fills the last wave of warp chunks (24 resident warps per SM): on the
+    1,048,576-row banded matrix, sigma 32 has 24,576 tiles; 7 per chunk make 3,511 chunks, one
+    wave on 148 SMs.  A wave form whose count equals the default is timed once."""
     torch = cuda
     A = M.banded(1_048_576, 64, 24, seed=3)
     warps = 24 * torch.cuda.get_device_properties(0).multi_processor_count
@@ -266,16 +267,24 @@ def test_autotune_wave_balanced_csr5(cuda):
         return 4 if tiles >= 4 * warps else (2 if tiles >= 2 * warps else 1)
 
     ents, best = autotune(A, k=1, reps=2)
+    assert len(ents) == _abi.NVARIANTS
     for sg in (16, 32):
         tiles = A.nnz // (32 * sg)
-        got = {e["opts"]["tiles_per_chunk"] for e in ents
-               if e["format"] == "csr5" and e["opts"]["sigma"] == sg}
-        want = {0} | ({wave(tiles)} if wave(tiles) != default(tiles) else set())
-        assert got == want, (sg, got, want)
+        es = [e for e in ents if e["format"] == "csr5" and e["opts"]["sigma"] == sg]
+        assert {e["opts"]["tiles_per_chunk"] for e in es} == {0, _abi.TILES_WAVE}
+        for tpc in (0, _abi.TILES_WAVE):
+            g = wave(tiles) if tpc == _abi.TILES_WAVE else default(tiles)
+            mat = SpMatrix(A, "csr5", sigma=sg, tiles_per_chunk=tpc)
+            assert mat.info()["elems_per_chunk"] == 32 * sg * g
+            mat.close()
+        if wave(tiles) == default(tiles):  # the same form: one timing for both entries
+            d = {e["opts"]["tiles_per_chunk"]: e["ms"] for e in es
+                 if e["opts"]["index_mode"] == _abi.INDEX_I32}
+            assert d[0] == d[_abi.TILES_WAVE]
     # the wave-balanced form computes the same product as the default one
     x = torch.from_numpy(M.uniform(A.n, seed=33)).cuda()
     y0 = SpMatrix(A, "csr5", sigma=32).spmv(x).cpu().numpy()
-    y1 = SpMatrix(A, "csr5", sigma=32, tiles_per_chunk=wave(A.nnz // 1024)).spmv(x).cpu().numpy()
+    y1 = SpMatrix(A, "csr5", sigma=32, tiles_per_chunk=_abi.TILES_WAVE).spmv(x).cpu().numpy()
     yr, ab = O.csr_ref(A.rp, A.ci, A.v, x.cpu().numpy())
     assert O.rel_error(y0, yr, ab, TOL)[0] == 0 and O.rel_error(y1, yr, ab, TOL)[0] == 0
 

@@ -17,7 +17,7 @@ def test_training_set_file():
     d = np.load(DATA)
     n = int(d["n_train"]) + int(d["n_test"])
     assert (int(d["n_train"]), int(d["n_test"])) == (2000, 200)
-    assert d["features"].shape == (n, 12) and d["times_ms"].shape == (n, 6)
+    assert d["features"].shape == (n, 12) and d["times_ms"].shape == (n, 30)
     assert np.isfinite(d["features"]).all()
     assert (d["times_ms"] > 0).mean() > 0.99          # nearly every variant ran
     assert np.all(np.bincount(d["family"], minlength=4) == n // 4)
@@ -45,8 +45,8 @@ def test_cpu_gradient_against_finite_differences():
     rng = np.random.default_rng(1)
     P = rng.normal(scale=0.3, size=R.NP)
     X = rng.normal(size=(50, 12))
-    T = rng.normal(size=(50, 6))
-    mask = (rng.uniform(size=(50, 6)) > 0.2).astype(float)
+    T = rng.normal(size=(50, R.OUT))
+    mask = (rng.uniform(size=(50, R.OUT)) > 0.2).astype(float)
     loss, g = R.mlp_loss_grad(P, X, T, mask)
     for p in rng.choice(R.NP, 40, replace=False):
         h = 1e-6
@@ -74,3 +74,38 @@ def test_cpu_features_small():
     assert np.isclose(f[7], 2 / 3)                     # two rows with 1..4 nonzeros
     assert np.isclose(f[10], (1 + 2) / 5)              # x lines: row 0 one, row 2 two
     assert np.isclose(f[9], 1.0)                       # all within 64 of the diagonal
+
+
+def test_form_space_matches_the_library():
+    """The 30 forms: pava_variant's formats and tile parameters, their kernel variant
+    (pava_variant_family), and the names and families the selector reports use."""
+    import ctypes
+    from pava_b200 import _abi
+    L = _abi.gpu()
+    assert len(S.FORM_NAMES) == _abi.NVARIANTS == R.OUT == _abi.MLP_OUT
+    seen = set()
+    for v in range(_abi.NVARIANTS):
+        f = ctypes.c_int()
+        o = _abi.PavaOpts()
+        assert L.pava_variant(v, ctypes.byref(f), ctypes.byref(o)) == 0
+        assert L.pava_variant_family(v) == S.FORM_FAMILY[v]
+        name = S.FORM_NAMES[v]
+        idx = "auto" if o.index_mode == _abi.INDEX_AUTO else "i32"
+        if f.value == _abi.FORMAT_CVR:
+            assert name == f"cvr_s{o.steps}_{idx}"
+        elif f.value == _abi.FORMAT_CSR5:
+            w = "tiles_wave" if o.tiles_per_chunk == _abi.TILES_WAVE else "tiles_default"
+            assert o.tiles_per_chunk in (0, _abi.TILES_WAVE)
+            assert name == f"csr5_s{o.sigma}_{w}_{idx}"
+        else:
+            assert f.value == _abi.FORMAT_CSR
+            groups = o.rows_per_tile // (32 // o.lanes_per_row)
+            assert name == f"csr_l{o.lanes_per_row}_g{groups}"
+        key = (f.value, o.steps, o.sigma, o.tiles_per_chunk, o.index_mode, o.lanes_per_row,
+               o.rows_per_tile)
+        assert key not in seen
+        seen.add(key)
+    assert L.pava_variant(30, None, None) == _abi.E_INVALID_ARG
+    assert L.pava_variant_family(-1) == -1
+    for fam, v in enumerate(S.FAMILY_DEFAULT_FORM):
+        assert S.FORM_FAMILY[v] == fam
