@@ -46,6 +46,9 @@ def parse():
     p.add_argument("--impl", choices=["pava", "reference"], default="pava")
     p.add_argument("--rows", type=int, default=4_194_304, help="smaller sizes for smoke runs")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-numa-local", dest="numa_local", action="store_false",
+                   help="allocate the end-to-end run's pinned host buffers wherever the process "
+                        "runs instead of on the GPU's NUMA node")
     p.add_argument("--no-precision", action="store_true",
                    help="skip the FP64 vs FP32C comparison on the 27-point stencil")
     p.add_argument("--variants", default="cvr:steps=64,cvr:steps=128,csr5:sigma=16,csr5:sigma=32",
@@ -142,6 +145,27 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_local_cpus(index):
+    """The CPUs of the NUMA node the GPU hangs off (sysfs local_cpulist of its PCI function),
+    limited to those this process may use; None when unknown."""
+    try:
+        import torch
+        p = torch.cuda.get_device_properties(index)
+        path = (f"/sys/bus/pci/devices/{p.pci_domain_id:04x}:{p.pci_bus_id:02x}:"
+                f"{p.pci_device_id:02x}.0/local_cpulist")
+        cpus = set()
+        for part in open(path).read().strip().split(","):
+            if "-" in part:
+                a, b = part.split("-")
+                cpus |= set(range(int(a), int(b) + 1))
+            elif part:
+                cpus.add(int(part))
+        cpus &= os.sched_getaffinity(0)
+        return cpus or None
+    except Exception:
+        return None
 
 
 def max_over_ranks(values, world, device):
@@ -333,8 +357,18 @@ def main():
     # end-to-end through the public host-buffer entry point: every step copies x in from pinned
     # host memory, runs the SpMV and copies y out (pava_spmv_host_async: consecutive steps
     # overlap one step's copy-in, another's SpMV and a third's copy-out)
-    xh = torch.from_numpy(x_host).pin_memory()
-    yh = torch.empty(A.m, dtype=torch.float64).pin_memory()
+    # the pinned buffers on the GPU's own NUMA node (the copies then cross one socket link)
+    saved = os.sched_getaffinity(0)
+    local = gpu_local_cpus(torch.cuda.current_device()) if args.numa_local else None
+    if local:
+        os.sched_setaffinity(0, local)
+    try:
+        xh = torch.from_numpy(x_host).pin_memory()
+        yh = torch.empty(A.m, dtype=torch.float64).pin_memory()
+        yh.zero_()
+    finally:
+        if local:
+            os.sched_setaffinity(0, saved)
     KE = max(3, K)
     for _ in range(2):
         mat.spmv_host_async(xh, yh, stream=stream)
@@ -397,7 +431,8 @@ def main():
             "e2e": {"value": round(aggregate_gbps(world, alg, e2e_ms), 3), "unit": "GB/s",
                     "ms_per_step": round(e2e_ms, 6), "steps": KE, "h2d_bytes_per_step": 8 * A.n,
                     "d2h_bytes_per_step": 8 * A.m, "entry_point": "pava_spmv_host_async",
-                    "y_equals_device_result": e2e_ok},
+                    "y_equals_device_result": e2e_ok,
+                    "pinned_on_gpu_numa_node": bool(local)},
             "gpu_launches": 2 * K,
             "clocks": clocks.summary(),
             "format_bytes_per_step": info["format_bytes"],

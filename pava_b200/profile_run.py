@@ -74,6 +74,9 @@ def main():
     p.add_argument("--k", type=int, default=1,
                    help="right-hand sides: k > 1 times pava_spmm on X (n x k, row-major); "
                         "CSR variants only")
+    p.add_argument("--floor-modes", default="0,1,2,3",
+                   help="floor kernels to run (0 streams, 1 gathers, 2 cols+gathers, 3 dot)")
+    p.add_argument("--floor-bps", default="2,4,8,16", help="blocks per SM to sweep")
     p.add_argument("--floor", action="store_true",
                    help="time the floor kernels (pava_probe.h) on the matrix instead")
     p.add_argument("--flush", action="store_true",
@@ -90,7 +93,9 @@ def main():
     A = make_matrix(a.matrix, a.rows, a.count)
     x64 = M.uniform(A.n, seed=1, fp32=True)
     if a.floor:
-        run_floors(torch, A, x64, max(a.reps, 3), a.quiet)
+        run_floors(torch, A, x64, max(a.reps, 1), a.quiet,
+                   [int(t) for t in a.floor_modes.split(",")],
+                   [int(t) for t in a.floor_bps.split(",")])
         return
     for fmt, kw in parse_variants(a.variants):
         prec = kw.get("precision", _abi.PREC_FP64)
@@ -145,7 +150,7 @@ FLOOR_MODES = {0: ("streams", 12), 1: ("gathers", 0), 2: ("cols+gathers", 4),
                3: ("vals+cols+gathers", 12)}
 
 
-def run_floors(torch, A, x_host, reps, quiet):
+def run_floors(torch, A, x_host, reps, quiet, modes=(0, 1, 2, 3), bps_list=(2, 4, 8, 16)):
     """Floor kernels over A's nonzeros in CSR order: the best of blocks per SM in {2, 4, 8, 16}
     (256 threads) for each mode, CUDA-event timed, x resident in L2 as in an SpMV loop."""
     from . import _abi
@@ -154,9 +159,10 @@ def run_floors(torch, A, x_host, reps, quiet):
     v = torch.from_numpy(A.v).cuda()
     x = torch.from_numpy(x_host).cuda()
     s = torch.cuda.current_stream().cuda_stream
-    for mode, (name, bpe) in FLOOR_MODES.items():
+    for mode in modes:
+        name, bpe = FLOOR_MODES[mode]
         best = None
-        for bps in (2, 4, 8, 16):
+        for bps in bps_list:
             out = torch.empty(P.pava_probe_floor_out_len(bps, 256), dtype=torch.float64,
                               device="cuda")
             args = (mode, v.data_ptr(), ci.data_ptr(), x.data_ptr(), A.nnz, A.n, 1, bps, 256,
