@@ -148,14 +148,6 @@ __device__ __forceinline__ void tile_combine(double head, double tail, bool seen
     }
 }
 
-// Fast paths: 1 = the bit test, park, slot step and restarts of an element share one
-// predicate (Acc<T>::step_parked); 0 = each is derived on its own
-#ifndef PAVA_F32_FUSED_STEP
-#define PAVA_F32_FUSED_STEP 1
-#endif
-#ifndef PAVA_F64_FUSED_STEP
-#define PAVA_F64_FUSED_STEP 0
-#endif
 #ifndef PAVA_CSR5_MINB32
 #define PAVA_CSR5_MINB32 3
 #endif
@@ -262,12 +254,6 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
             }
             const unsigned Fb = F >> (qb * 4);
             if (fast) {  // row ends park the piece in the lane's shared slots: no branch
-#if PAVA_F64_FUSED_STEP
-                acc.template step_parked<SLOT, 1u>(Fb, sp, v0.get(0), x0[0]);
-                acc.template step_parked<SLOT, 2u>(Fb, sp, v0.get(1), x0[1]);
-                acc.template step_parked<SLOT, 4u>(Fb, sp, v0.get(2), x0[2]);
-                acc.template step_parked<SLOT, 8u>(Fb, sp, v0.get(3), x0[3]);
-#else
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const bool st = (Fb >> q) & 1u;
@@ -275,7 +261,6 @@ csr5_spmv_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ tile_
                     sp += st ? SLOT : 0u;
                     acc.add_restart(v0.get(q), x0[q], st);
                 }
-#endif
             } else {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -436,13 +421,6 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
                                         : c1.gather_all(q, xb, pl, xlo, xhi, err);
                     }
                     if (FAST) {  // row ends park the piece in the lane's shared slots
-#if PAVA_F32_FUSED_STEP
-                        const unsigned Fq = F >> (qb * 4);
-                        acc.template step_parked<SLOT, 1u>(Fq, sp, v0.get(0), x0[0]);
-                        acc.template step_parked<SLOT, 2u>(Fq, sp, v0.get(1), x0[1]);
-                        acc.template step_parked<SLOT, 4u>(Fq, sp, v0.get(2), x0[2]);
-                        acc.template step_parked<SLOT, 8u>(Fq, sp, v0.get(3), x0[3]);
-#else
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
                             const bool st = (F >> (qb * 4 + q)) & 1u;
@@ -450,7 +428,6 @@ csr5_spmv_f32_kernel(const ChunkHdr *__restrict__ hdr, const int *__restrict__ t
                             sp += st ? SLOT : 0u;
                             acc.add_restart(v0.get(q), x0[q], st);
                         }
-#endif
                     } else {
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {

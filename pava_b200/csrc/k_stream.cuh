@@ -148,20 +148,6 @@ template <> struct Acc<double> {
     }
     double s = 0.0;
     __device__ __forceinline__ void add(double v, double x) { s = fma(v, x, s); }
-    // Acc<float>::step_parked for FP64: park s at sp when the bit is set, step sp, restart.
-    template <unsigned SLOT, unsigned MASK>
-    __device__ __forceinline__ void step_parked(unsigned F, unsigned &sp, double v, double x) {
-        asm volatile(
-            "{ .reg .pred q; .reg .b32 t;\n\t"
-            "and.b32 t, %2, %3;\n\t"
-            "setp.ne.u32 q, t, 0;\n\t"
-            "@q st.shared.f64 [%0], %1;\n\t"
-            "@q add.u32 %0, %0, %4;\n\t"
-            "selp.f64 %1, 0d0000000000000000, %1, q; }"
-            : "+r"(sp), "+d"(s)
-            : "r"(F), "n"(MASK), "n"(SLOT));
-        s = fma(v, x, s);
-    }
     __device__ __forceinline__ double value() const { return s; }
     __device__ __forceinline__ void reset() { s = 0.0; }
 };
@@ -186,24 +172,6 @@ template <> struct Acc<float> {
     __device__ __forceinline__ void add_restart(float v, float x, bool st) {
         s = st ? 0.f : s;
         c = st ? 0.f : c;
-        add(v, x);
-    }
-    // One element of the branch-free row walk: when the MASK bit of the lane's row-start mask
-    // F is set, the element starts a row, so the finished piece (s, c) is parked at the shared
-    // address sp, sp moves to the lane's next slot and the sums restart; then v*x is added.
-    // The bit test, the park, the slot step and both restarts share one predicate.
-    template <unsigned SLOT, unsigned MASK>
-    __device__ __forceinline__ void step_parked(unsigned F, unsigned &sp, float v, float x) {
-        asm volatile(
-            "{ .reg .pred q; .reg .b32 t;\n\t"
-            "and.b32 t, %3, %4;\n\t"
-            "setp.ne.u32 q, t, 0;\n\t"
-            "@q st.shared.v2.f32 [%0], {%1, %2};\n\t"
-            "@q add.u32 %0, %0, %5;\n\t"
-            "selp.f32 %1, 0f00000000, %1, q;\n\t"
-            "selp.f32 %2, 0f00000000, %2, q; }"
-            : "+r"(sp), "+f"(s), "+f"(c)
-            : "r"(F), "n"(MASK), "n"(SLOT));
         add(v, x);
     }
     __device__ __forceinline__ double value() const { return (double)s + (double)c; }
