@@ -509,7 +509,7 @@ def precision_form(torch, stream):
     """The precision form on the 128^3 27-point stencil (2,097,152 rows, 55.7 M nnz, values and
     x FP32-representable): the fastest FP64 form against the fastest FP32C form (FP32 values
     and x, 16-bit column offsets, compensated FP32 accumulation, FP64 carries) of the same
-    small sweep (CSR5 sigma 32 with 4 and 8 tiles per chunk; CVR steps 128), each timed as
+    small sweep (CSR5 sigma 32 with 4 and 8 tiles per chunk; CVR steps 128; SELL), each timed as
     whole SpMVs (kernel + carry fixup) back to back, 30 after 5 warm-ups; the FP32C result's
     relative error per row against the FP64 result (cancellation-aware denominator)."""
     from pava_b200 import _abi
@@ -522,7 +522,7 @@ def precision_form(torch, stream):
         x64 = torch.from_numpy(xh).cuda()
         x32 = x64.float()
         sweep = [("csr5", dict(sigma=32)), ("csr5", dict(sigma=32, tiles_per_chunk=8)),
-                 ("cvr", dict(steps=128))]
+                 ("cvr", dict(steps=128)), ("sell", dict())]
         out, ys = {}, {}
         for prec, x, extra in ((_abi.PREC_FP64, x64, {}),
                                (_abi.PREC_FP32C, x32, dict(index_mode=_abi.INDEX_DELTA16))):
@@ -541,6 +541,8 @@ def precision_form(torch, stream):
                 b.synchronize()
                 ms = a.elapsed_time(b) / 30
                 name = fmt + "".join(f"_{k}{v}" for k, v in kw.items())
+                out.setdefault("sweep_ms", {})[f"{'fp64' if prec == _abi.PREC_FP64 else 'fp32c'}"
+                                               f" {name}"] = round(ms, 6)
                 if best is None or ms < best[1]:
                     best = (name, ms)
                     ys[prec] = y.cpu().numpy()

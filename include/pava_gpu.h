@@ -42,7 +42,11 @@ typedef enum pava_status {
 typedef enum pava_format {
     PAVA_FORMAT_CSR = 0,   /* plain CSR, row-group kernel (lanes per row, SpMM, batches) */
     PAVA_FORMAT_CSR5 = 1,  /* CSR5 tiles: 32 lanes x sigma, bit-flag descriptors */
-    PAVA_FORMAT_CVR = 3    /* CVR chunks: 32 lanes x S steps, row-completion bits */
+    PAVA_FORMAT_CVR = 3,   /* CVR chunks: 32 lanes x S steps, row-completion bits */
+    PAVA_FORMAT_SELL = 4   /* sliced ELLPACK: slices of 32 rows, one lane per row, rows padded
+                              to the slice's longest (rounded up to 4); refused
+                              (PAVA_E_UNSUPPORTED_PARAMS) when padding would more than double
+                              the stored elements.  No counterpart in the reference. */
 } pava_format;
 
 typedef enum pava_precision {

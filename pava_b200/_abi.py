@@ -33,7 +33,7 @@ E_NOMEM = -13
 E_TIMEOUT = -14
 E_TOO_LARGE = -15
 
-FORMAT_CSR, FORMAT_CSR5, FORMAT_CVR = 0, 1, 3
+FORMAT_CSR, FORMAT_CSR5, FORMAT_CVR, FORMAT_SELL = 0, 1, 3, 4
 PREC_FP64, PREC_FP32C = 0, 1
 INDEX_I32, INDEX_DELTA16, INDEX_AUTO = 0, 1, 2
 

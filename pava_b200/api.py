@@ -19,7 +19,8 @@ import numpy as np
 from . import _abi
 from .matrices import CSR
 
-FORMATS = {"csr": _abi.FORMAT_CSR, "csr5": _abi.FORMAT_CSR5, "cvr": _abi.FORMAT_CVR}
+FORMATS = {"csr": _abi.FORMAT_CSR, "csr5": _abi.FORMAT_CSR5, "cvr": _abi.FORMAT_CVR,
+           "sell": _abi.FORMAT_SELL}
 
 
 def _torch():
@@ -35,7 +36,7 @@ def _stream_ptr(stream) -> int | None:
 
 
 class SpMatrix:
-    """A CSR matrix converted on the GPU into ``format`` ('cvr', 'csr5' or 'csr').
+    """A CSR matrix converted on the GPU into ``format`` ('cvr', 'csr5', 'sell' or 'csr').
 
     ``spmv(x)`` takes a CUDA tensor (float64 for FP64 handles) and returns y (float64).
     ``spmv_host(x)`` is the end-to-end form on host arrays.

@@ -252,6 +252,50 @@ pava_status convert(pava::Handle &h, const int *rp, const int *ci, const double 
         if (ovf)
             return fail(PAVA_E_UNSUPPORTED_PARAMS,
                         "16-bit column offsets: a chunk's columns span more than 65534");
+    } else if (h.format == PAVA_FORMAT_SELL) {  // slices of 32 rows, padded, block layout
+        h.nchunks = ((long long)h.m + 31) / 32;
+        h.L = 32;
+        h.meta_stride = sizeof(pava::SellSlice);
+        PAVA_CUDA(dalloc((pava::SellSlice **)&h.meta, (size_t)h.nchunks, &h.device_bytes),
+                  "cudaMalloc(slices)");
+        int *d_off = nullptr, *d_tot = nullptr, *d_ovf = nullptr;
+        int total_blk = 0, ovf = 0;
+        cudaError_t e = cudaMallocAsync(&d_off, sizeof(int) * (size_t)(h.nchunks + 1), s);
+        if (e == cudaSuccess) e = cudaMallocAsync(&d_tot, sizeof(int), s);
+        if (e == cudaSuccess) e = cudaMallocAsync(&d_ovf, sizeof(int), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_ovf, 0, sizeof(int), s);
+        if (e == cudaSuccess && h.nchunks > 0) e = pava::sell_plan(h, rp, ci, d_off, d_tot, s);
+        if (e == cudaSuccess && h.nchunks > 0)
+            e = cudaMemcpyAsync(&total_blk, d_tot, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        const long long padded = (long long)total_blk * 128;
+        pava_status st = PAVA_SUCCESS;
+        if (e != cudaSuccess) {
+            st = fail_cuda(e, "SELL plan");
+        } else if (padded > 2LL * h.nnz + 128LL * h.nchunks) {
+            st = fail(PAVA_E_UNSUPPORTED_PARAMS,
+                      "SELL: padding the slices would more than double the stored elements (" +
+                          std::to_string(padded) + " for " + std::to_string(h.nnz) + " nonzeros)");
+        } else if (padded >= (long long)INT_MAX - 64) {
+            st = fail(PAVA_E_TOO_LARGE, "SELL: padded elements exceed the int32 element space");
+        } else {
+            h.n_aug = padded;
+            e = budget_malloc(&h.vals, sv * (size_t)(padded ? padded : 1), &h.device_bytes);
+            if (e == cudaSuccess)
+                e = budget_malloc(&h.cols, si * (size_t)(padded ? padded : 1), &h.device_bytes);
+            if (e == cudaSuccess && h.nchunks > 0) e = pava::sell_fill(h, rp, ci, v, d_off, d_ovf, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&ovf, d_ovf, sizeof(int), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) st = fail_cuda(e, "SELL conversion");
+        }
+        cudaFreeAsync(d_off, s);
+        cudaFreeAsync(d_tot, s);
+        cudaFreeAsync(d_ovf, s);
+        if (st != PAVA_SUCCESS) return st;
+        h.d16_overflow = ovf ? 1 : 0;
+        if (ovf)
+            return fail(PAVA_E_UNSUPPORTED_PARAMS,
+                        "16-bit column offsets: a slice's columns span more than 65534");
     } else {  // plain CSR: private copies (values narrowed to float for FP32C)
         PAVA_CUDA(dalloc(&h.rp, (size_t)h.m + 1, &h.device_bytes), "cudaMalloc(rp)");
         PAVA_CUDA(dalloc(&h.ci, (size_t)h.nnz, &h.device_bytes), "cudaMalloc(ci)");
@@ -375,7 +419,8 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
     if (!out) return fail(PAVA_E_INVALID_ARG, "out is NULL");
     *out = nullptr;
     if (!A) return fail(PAVA_E_INVALID_ARG, "matrix is NULL");
-    if (format != PAVA_FORMAT_CSR && format != PAVA_FORMAT_CSR5 && format != PAVA_FORMAT_CVR)
+    if (format != PAVA_FORMAT_CSR && format != PAVA_FORMAT_CSR5 && format != PAVA_FORMAT_CVR &&
+        format != PAVA_FORMAT_SELL)
         return fail(PAVA_E_UNKNOWN_FORMAT, "unknown format");
     if (A->m < 0 || A->n < 0 || A->nnz < 0) return fail(PAVA_E_INVALID_ARG, "negative size");
     if (!A->row_ptr || (A->nnz > 0 && (!A->col_idx || !A->vals)))
@@ -442,6 +487,8 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
             return fail(PAVA_E_UNSUPPORTED_PARAMS, "CSR5 sigma must be 8/12/16/24/32, tiles 1..64");
         }
         h.L = 32LL * h.sigma * h.G;
+    } else if (format == PAVA_FORMAT_SELL) {
+        // no shape options: a slice is 32 rows, its block 4 steps
     } else {
         // 0 = derive per call (resolve_group_shape)
         h.lanes_per_row = o.lanes_per_row;
@@ -551,6 +598,8 @@ pava_status pava_spmv_stage(pava_handle *H, const void *x, void *y, void *stream
     } else if (h.format == PAVA_FORMAT_CSR5) {
         if (main_k) e = pava::csr5_spmv(h, x, y, s);
         if (e == cudaSuccess && fix_k) e = pava::carry_fixup(h, y, s);
+    } else if (h.format == PAVA_FORMAT_SELL) {  // one pass: every row ends in its own lane
+        if (main_k) e = pava::sell_spmv(h, x, y, s);
     } else {
         if (main_k) {
             pava::Handle g;
@@ -665,6 +714,9 @@ pava_status pava_get_info(const pava_handle *H, pava_info *out) {
     else if (h.format == PAVA_FORMAT_CSR5)
         out->format_bytes = (double)h.nchunks * h.L * (sv + si) + (double)h.ntiles * (32 * 4 + 4) +
                             (double)h.nchunks * sizeof(pava::ChunkHdr) + xy;
+    else if (h.format == PAVA_FORMAT_SELL)  // padded slices and their descriptors
+        out->format_bytes = (double)h.n_aug * (sv + si) +
+                            (double)h.nchunks * sizeof(pava::SellSlice) + xy;
     else
         out->format_bytes = (double)h.nnz * (sv + si) + 4.0 * ((double)h.m + 1) + xy;
     return PAVA_SUCCESS;
@@ -700,7 +752,10 @@ int conduct_gpu(int format, int m, int n, int nnz, const int *rp, const int *ci,
         rec->status = PAVA_E_INVALID_ARG;
         rec->convert_s = rec->exec_s = -1.0;
     }
-    const char *fname = format == PAVA_FORMAT_CVR ? "CVR" : (format == PAVA_FORMAT_CSR5 ? "CSR5" : "CSR");
+    const char *fname = format == PAVA_FORMAT_CVR    ? "CVR"
+                        : format == PAVA_FORMAT_CSR5 ? "CSR5"
+                        : format == PAVA_FORMAT_SELL ? "SELL"
+                                                     : "CSR";
     int st = pava_create(&A, format, &o, nullptr, &H);
     if (st != PAVA_SUCCESS) {
         printf(" Performance %s %s %d %f %f \n", name ? name : "", fname, 0, -1.0, -1.0);

@@ -28,6 +28,15 @@ struct CvrMeta {
 };
 static_assert(sizeof(CvrMeta) == 128, "CvrMeta layout");
 
+// Per-slice descriptor of the SELL form (32 rows; 4-step blocks of 128 elements).
+struct SellSlice {
+    int off;         // first element of the slice in the value and column streams
+    int nblk;        // 4-step blocks: the slice's longest row, rounded up to 4, over 4
+    int colbase;     // DELTA16: base column of the 16-bit offsets
+    unsigned flags;  // bit 0: some row of the slice is padded (padding reads no x)
+};
+static_assert(sizeof(SellSlice) == 16, "SellSlice layout");
+
 // Engine handle (behind the opaque pava_handle of the C ABI).
 struct Handle {
     int format = 0, precision = 0, index_mode = 0;
@@ -110,6 +119,15 @@ cudaError_t csr5_convert(Handle &h, const int *rp, const int *ci, const double *
 cudaError_t csr5_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
 
 cudaError_t carry_fixup(const Handle &h, void *y, cudaStream_t s);
+
+// SELL: sell_plan fills the slice descriptors (h.meta, h.nchunks slices) except their offsets
+// and writes the exclusive scan of the slices' block counts to d_blk_off[0..nslices], the total
+// to *d_total_blk; sell_fill writes the padded streams and the offsets.
+cudaError_t sell_plan(Handle &h, const int *rp, const int *ci, int *d_blk_off, int *d_total_blk,
+                      cudaStream_t s);
+cudaError_t sell_fill(Handle &h, const int *rp, const int *ci, const double *v,
+                      const int *d_blk_off, int *ovf, cudaStream_t s);
+cudaError_t sell_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
 
 // Plain CSR row-group kernel: y = A x, and Y = A X with X row-major n x k (leading
 // dimensions ldx, ldy in elements).

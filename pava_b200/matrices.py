@@ -128,6 +128,21 @@ def init_vectors(m: int, n: int):
     return x, y, yr
 
 
+def sell_padded_elements(A: CSR) -> int:
+    """Elements the SELL form stores for A: per slice of 32 rows (the last one filled up with
+    empty rows), 32 x its longest row rounded up to a multiple of 4."""
+    lens = np.diff(np.asarray(A.rp, np.int64))
+    ns = (A.m + 31) // 32
+    lens = np.concatenate([lens, np.zeros(ns * 32 - A.m, np.int64)]).reshape(ns, 32)
+    return int(((lens.max(axis=1) + 3) // 4).sum()) * 128 if ns else 0
+
+
+def sell_accepts(A: CSR) -> bool:
+    """Whether pava_create takes A in the SELL form: its padding at most doubles the stored
+    elements (plus one block of 128 per slice), PAVA_E_UNSUPPORTED_PARAMS otherwise."""
+    return sell_padded_elements(A) <= 2 * A.nnz + 128 * ((A.m + 31) // 32)
+
+
 def from_arrays(m, n, rp, ci, v) -> CSR:
     return CSR(int(m), int(n), np.ascontiguousarray(rp, np.int32),
                np.ascontiguousarray(ci, np.int32), np.ascontiguousarray(v, np.float64))

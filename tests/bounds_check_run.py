@@ -55,8 +55,24 @@ def main():
         else:
             worst = max(worst, e)
         mat.close()
-    # multi-RHS through the X-window kernel
+    # SELL (the power-law matrix pads too much for it) on a banded matrix and a stencil
     B = M.banded(20_000, 64, 24, seed=93)
+    for S, kw in ((B, {}), (B, dict(precision=_abi.PREC_FP32C, index_mode=_abi.INDEX_AUTO)),
+                  (M.stencil27(24, seed=96), dict(index_mode=_abi.INDEX_DELTA16))):
+        S = M.from_arrays(S.m, S.n, S.rp, S.ci, S.v.astype(np.float32).astype(np.float64))
+        xs_ = M.uniform(S.n, seed=97, fp32=True)
+        fp32 = kw.get("precision") == _abi.PREC_FP32C
+        mat = SpMatrix(S, "sell", **kw)
+        xd = torch.from_numpy(xs_).to("cuda", torch.float32 if fp32 else torch.float64)
+        y = mat.spmv(xd).cpu().numpy()
+        ysr, absr = O.csr_ref(S.rp, S.ci, S.v, xs_)
+        e = O.rel_error(y, ysr, absr, 1e-9 if fp32 else 1e-12)[1]
+        if fp32:
+            worst32 = max(worst32, e)
+        else:
+            worst = max(worst, e)
+        mat.close()
+    # multi-RHS through the X-window kernel
     X = M.uniform(B.n * 8, seed=94).reshape(B.n, 8)
     Y = SpMatrix(B, "csr", lanes_per_row=8, col_lanes=8, x_window=1).spmm(
         torch.from_numpy(X).cuda()).cpu().numpy()

@@ -83,6 +83,16 @@ def test_powerlaw_full_size_bench_forms(cuda, powerlaw_c2, fmt, kw):
     _assert_all(y, oracles, ab, TOL, f"{fmt} {kw}")
 
 
+def test_powerlaw_full_size_sell_refused(cuda, powerlaw_c2):
+    """Padding every 32-row slice of the lognormal rows to its longest row would store ~10x
+    the nonzeros: the SELL form refuses the matrix instead of converting it."""
+    A = powerlaw_c2[0]
+    assert not M.sell_accepts(A) and M.sell_padded_elements(A) > 8 * A.nnz
+    with pytest.raises(_abi.PavaError) as e:
+        SpMatrix(A, "sell")
+    assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
+
+
 @pytest.fixture(scope="module")
 def stencil_c3():
     A = M.stencil27(128, seed=2)
@@ -93,8 +103,8 @@ def stencil_c3():
 
 
 C3_FORMS = [("csr5", dict(sigma=32)), ("csr5", dict(sigma=32, tiles_per_chunk=8)),
-            ("cvr", dict(steps=128))]
-C3_IDS = ["csr5_sigma32", "csr5_sigma32_tiles_per_chunk8", "cvr_steps128"]
+            ("cvr", dict(steps=128)), ("sell", dict())]
+C3_IDS = ["csr5_sigma32", "csr5_sigma32_tiles_per_chunk8", "cvr_steps128", "sell"]
 
 
 @pytest.mark.parametrize("fmt,kw", C3_FORMS, ids=C3_IDS)

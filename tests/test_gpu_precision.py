@@ -17,8 +17,18 @@ pytestmark = pytest.mark.gpu
 
 TOL32 = 1e-9
 FORMS = [("cvr", dict(steps=64)), ("cvr", dict(steps=128)), ("csr5", dict(sigma=16)),
-         ("csr5", dict(sigma=32, tiles_per_chunk=2))]
-FID = ["cvr64", "cvr128", "csr5s16", "csr5s32"]
+         ("csr5", dict(sigma=32, tiles_per_chunk=2)), ("sell", dict())]
+FID = ["cvr64", "cvr128", "csr5s16", "csr5s32", "sell"]
+
+
+def _refused(A, fmt, **kw):
+    """True (after checking the refusal) where the SELL form must refuse A for its padding."""
+    if fmt != "sell" or M.sell_accepts(A):
+        return False
+    with pytest.raises(_abi.PavaError) as e:
+        SpMatrix(A, fmt, **kw)
+    assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
+    return True
 
 
 def _run(torch, A, x, fmt, precision, index_mode, **kw):
@@ -48,6 +58,8 @@ def test_fp32c_irregular(cuda, fmt, kw):
     A = M.powerlaw(200_000, mean=16.0, cap=50_000, seed=5)
     A.v = A.v.astype(np.float32).astype(np.float64)
     x = M.uniform(A.n, seed=6, fp32=True)
+    if _refused(A, fmt, precision=_abi.PREC_FP32C, **kw):
+        return
     y, _ = _run(cuda, A, x, fmt, _abi.PREC_FP32C, _abi.INDEX_I32, **kw)
     yr, ab = O.csr_ref(A.rp, A.ci, A.v, x)
     bad, mx, _ = O.rel_error(y, yr, ab, TOL32)
@@ -110,7 +122,7 @@ def test_config3_full_size_fp32c_vs_fp64(cuda):
     y64, m64 = _run(cuda, A, x, "csr5", _abi.PREC_FP64, _abi.INDEX_I32)
     assert O.rel_error(y64, yr, ab, 1e-12)[0] == 0
     del m64
-    for fmt in ("cvr", "csr5"):
+    for fmt in ("cvr", "csr5", "sell"):
         y32, m32 = _run(cuda, A, x, fmt, _abi.PREC_FP32C, _abi.INDEX_DELTA16)
         bad, mx, mean = O.rel_error(y32, yr, ab, TOL32)
         assert bad == 0, (fmt, mx, mean)
@@ -172,7 +184,10 @@ def test_index_auto_picks_16_bit_where_it_fits(cuda, fmt, kw):
     reach; results bitwise equal to the 32-bit form either way."""
     torch = cuda
     for A, want in ((M.stencil27(30, seed=9), _abi.INDEX_DELTA16),
-                    (M.powerlaw(300_000, mean=12.0, seed=10), _abi.INDEX_I32)):
+                    (M.powerlaw(300_000, mean=12.0, seed=10), _abi.INDEX_I32),
+                    (M.random_csr(30_000, 300_000, 6.0, seed=16), _abi.INDEX_I32)):
+        if _refused(A, fmt, index_mode=_abi.INDEX_AUTO, **kw):
+            continue
         x = torch.from_numpy(M.uniform(A.n, seed=11)).cuda()
         auto = SpMatrix(A, fmt, index_mode=_abi.INDEX_AUTO, **kw)
         assert auto.info()["index_mode"] == want
