@@ -51,8 +51,9 @@ typedef enum pava_format {
 
 typedef enum pava_precision {
     PAVA_PREC_FP64 = 0,    /* values, x, y FP64; FMA accumulation */
-    PAVA_PREC_FP32C = 1    /* values and x FP32, compensated FP32 accumulation, FP64 carries
-                              and FP64 y */
+    PAVA_PREC_FP32C = 1    /* values and x FP32, FP64 y.  CVR / CSR5: compensated FP32
+                              accumulation, FP64 carries; SELL: the exact FP32 products
+                              summed in FP64 */
 } pava_precision;
 
 typedef enum pava_index_mode {

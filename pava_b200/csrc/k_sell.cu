@@ -26,9 +26,6 @@ namespace pava {
 namespace {
 
 constexpr int SELL_WARPS = 8;
-#ifndef PAVA_SELL_MINB
-#define PAVA_SELL_MINB 3
-#endif
 
 template <typename IT> __device__ __forceinline__ IT sell_enc(int col, int base, int *ovf);
 template <> __device__ __forceinline__ int sell_enc<int>(int col, int, int *) { return col; }
@@ -102,17 +99,62 @@ __global__ void sell_fill_kernel(const int *__restrict__ rp, const int *__restri
     if (lane == 0) meta[s].off = (int)off;
 }
 
+// Pipeline depth (blocks of 4 steps the value and column loads run ahead of their use) and
+// resident CTAs per SM of each value form.
+#ifndef PAVA_SELL_D64
+#define PAVA_SELL_D64 2
+#endif
+#ifndef PAVA_SELL_D32
+#define PAVA_SELL_D32 2
+#endif
+#ifndef PAVA_SELL_MINB64
+#define PAVA_SELL_MINB64 3
+#endif
+#ifndef PAVA_SELL_MINB32
+#define PAVA_SELL_MINB32 4
+#endif
+
+// Row sums.  FP64: FMA.  FP32 values and x: a product of two FP32 numbers is exact in FP64
+// (24 + 24 significant bits < 53), so the FP32 form widens both factors and sums the exact
+// products with FP64 FMAs -- an FP64 sum of exact terms, one rounding per nonzero.
+template <typename VT> struct RowAcc;
+template <> struct RowAcc<double> {
+    double s = 0.0;
+    __device__ __forceinline__ void add(double v, double x) { s = fma(v, x, s); }
+    __device__ __forceinline__ double value() const { return s; }
+    __device__ __forceinline__ void reset() { s = 0.0; }
+};
+template <> struct RowAcc<float> {
+    double s = 0.0;
+    __device__ __forceinline__ void add(float v, float x) { s = fma((double)v, (double)x, s); }
+    __device__ __forceinline__ double value() const { return s; }
+    __device__ __forceinline__ void reset() { s = 0.0; }
+};
+
+template <typename VT> struct SellShape;
+template <> struct SellShape<double> {
+    static constexpr int D = PAVA_SELL_D64, MINB = PAVA_SELL_MINB64;
+};
+template <> struct SellShape<float> {
+    static constexpr int D = PAVA_SELL_D32, MINB = PAVA_SELL_MINB32;
+};
+
 template <bool B> struct SFlag { static constexpr bool value = B; };
 
-// SpMV: one warp per slice (grid-stride over slices, persistent grid).  The slice's blocks run
-// through a register pipeline -- values two blocks ahead, columns three, x one -- and each lane
-// accumulates its own row; the slice ends with one coalesced store of 32 rows.
+// SpMV: one warp per slice (grid-stride over slices, persistent grid: the warps of the grid
+// work on neighbouring slices at any time, so the streams are read close to in order).  The
+// slice's blocks run through register rings of D slots: the values of block b + D and the
+// columns of block b + D + 1 are loaded while block b is summed and the x of block b + 1 is
+// gathered.  Each lane accumulates its own row; the slice ends with one coalesced store of 32
+// rows.
 template <typename VT, typename IT>
-__global__ void __launch_bounds__(SELL_WARPS * 32, PAVA_SELL_MINB)
+__global__ void __launch_bounds__(SELL_WARPS * 32, SellShape<VT>::MINB)
 sell_spmv_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals,
                  const IT *__restrict__ cols, const VT *__restrict__ x,
                  double *__restrict__ y, long long nslices, int m, int n,
                  unsigned long long *err) {
+    constexpr int D = SellShape<VT>::D;
+    static_assert(D >= 2 && D % 2 == 0, "the x ring of two slots needs an even depth");
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
     const long long nwarps = (long long)gridDim.x * SELL_WARPS;
@@ -124,7 +166,7 @@ sell_spmv_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
         const int xbase = sizeof(IT) == 2 ? S.colbase : 0;  // base of the 16-bit offsets
         const VT *xb = x + xbase;
         const int xlo = -xbase, xhi = n - xbase;
-        Acc<VT> acc;
+        RowAcc<VT> acc;
         // CHK: the slice pads some rows, so each gather tests its column
         auto walk = [&](auto chk_tag) {
             constexpr bool CHK = decltype(chk_tag)::value;
@@ -134,29 +176,34 @@ sell_spmv_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
                     xs[q] = CHK ? cbk.gather(q, xb, pl, xlo, xhi, err)
                                 : cbk.gather_all(q, xb, pl, xlo, xhi, err);
             };
-            CBlk<IT> c1 = CBlk<IT>::load(cb, NB > 1 ? 1 : 0, lane, pf);
-            CBlk<IT> c2 = CBlk<IT>::load(cb, NB > 2 ? 2 : 0, lane, pf);
-            VBlk<VT> v0 = VBlk<VT>::load(vb, 0, lane, pf);
-            VBlk<VT> v1 = VBlk<VT>::load(vb, NB > 1 ? 1 : 0, lane, pf);
-            VT x0[4];
-            {
-                const CBlk<IT> c0 = CBlk<IT>::load(cb, 0, lane, pf);
-                gather4(c0, x0);
+            VBlk<VT> v[D];
+            CBlk<IT> c[D];
+            VT xs[2][4];
+#pragma unroll
+            for (int j = 0; j < D; ++j) {
+                if (j < NB) {
+                    v[j] = VBlk<VT>::load(vb, j, lane, pf);
+                    c[j] = CBlk<IT>::load(cb, j, lane, pf);
+                }
             }
+            gather4(c[0], xs[0]);
+            if (D < NB) c[0] = CBlk<IT>::load(cb, D, lane, pf);
 #pragma unroll 1
-            for (int blk = 0; blk < NB; ++blk) {
-                CBlk<IT> cn = c2;
-                VBlk<VT> vn = v1;
-                if (blk + 3 < NB) cn = CBlk<IT>::load(cb, blk + 3, lane, pf);
-                if (blk + 2 < NB) vn = VBlk<VT>::load(vb, blk + 2, lane, pf);
-                VT x1[4];
-                if (blk + 1 < NB) gather4(c1, x1);
+            for (int b0 = 0; b0 < NB; b0 += D) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc.add(v0.get(q), x0[q]);
-                c1 = c2; c2 = cn;
-                v0 = v1; v1 = vn;
+                for (int j = 0; j < D; ++j) {  // block b = b0 + j sits in slot j
+                    const int b = b0 + j;
+                    if (b < NB) {
+                        const int jn = (j + 1) % D;  // slot of block b + 1
+                        if (b + 1 < NB) {
+                            gather4(c[jn], xs[(j + 1) & 1]);
+                            if (b + 1 + D < NB) c[jn] = CBlk<IT>::load(cb, b + 1 + D, lane, pf);
+                        }
 #pragma unroll
-                for (int q = 0; q < 4; ++q) x0[q] = x1[q];
+                        for (int q = 0; q < 4; ++q) acc.add(v[j].get(q), xs[j & 1][q]);
+                        if (b + D < NB) v[j] = VBlk<VT>::load(vb, b + D, lane, pf);
+                    }
+                }
             }
         };
         if (NB > 0) {
@@ -181,7 +228,7 @@ cudaError_t fill_t(Handle &h, const int *rp, const int *ci, const double *v, con
 template <typename VT, typename IT>
 cudaError_t spmv_t(const Handle &h, const void *x, void *y, cudaStream_t s) {
     const long long want = (h.nchunks + SELL_WARPS - 1) / SELL_WARPS;
-    const long long cap = (long long)h.sm_count * PAVA_SELL_MINB;
+    const long long cap = (long long)h.sm_count * SellShape<VT>::MINB;
     const unsigned grid = (unsigned)(want < cap ? want : cap);
     sell_spmv_kernel<VT, IT><<<grid, SELL_WARPS * 32, 0, s>>>(
         (const SellSlice *)h.meta, (const VT *)h.vals, (const IT *)h.cols, (const VT *)x,
