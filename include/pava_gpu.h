@@ -140,6 +140,14 @@ unsigned long long pava_get_device_memory_limit(void);
 int pava_bounds_checked(void);
 pava_status pava_bounds_report(unsigned long long *out3, int clear);
 
+/* Bounded waits.  The SELL SpMV waits on mbarriers for its bulk copies into shared memory;
+ * each wait gives up after about a second, counts itself in a device word and lets the kernel
+ * finish instead of hanging.  pava_wait_report(out2, clear) synchronises the device and
+ * returns PAVA_E_TIMEOUT when a wait gave up since the last clear (PAVA_SUCCESS otherwise),
+ * with out2 = {waits that gave up, the first one's slice + 1}; `clear` resets the word.  No
+ * reference counterpart (the reference's CPU code never waits on the device). */
+pava_status pava_wait_report(unsigned long long *out2, int clear);
+
 /* Converts A into `format` on the device (the GPU form of anonymouslibHandle::inputCSR +
  * asCSR5, csr5/anonymouslib_avx512.h:58-70,107-221, and of CVR's pre_processing,
  * cvr/cvr.h:583-1060).  The caller's arrays are never modified (the reference transposes

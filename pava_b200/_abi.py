@@ -91,6 +91,7 @@ GPU_SYMBOLS = [
     ("pava_set_device_memory_limit", c_int, [ctypes.c_ulonglong]),
     ("pava_bounds_checked", c_int, []),
     ("pava_bounds_report", c_int, [c_void_p, c_int]),
+    ("pava_wait_report", c_int, [c_void_p, c_int]),
     ("pava_get_device_memory_limit", ctypes.c_ulonglong, []),
     ("pava_create", c_int, [ctypes.POINTER(PavaCsr), c_int, ctypes.POINTER(PavaOpts), c_void_p,
                             ctypes.POINTER(c_void_p)]),

@@ -330,8 +330,28 @@ std::mutex g_guard_mutex;
 }  // namespace
 #endif
 
+// The bounded-wait word: [0] waits that gave up, [1] site of the first + 1 (SELL: its slice).
+__device__ unsigned long long g_wait_word[2];
+namespace {
+constexpr int WAIT_MAX_DEVICES = 64;
+void *g_wait_addr[WAIT_MAX_DEVICES] = {};
+std::mutex g_wait_mutex;
+}  // namespace
+
 namespace pava {
 void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+unsigned long long *wait_word() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= WAIT_MAX_DEVICES) return nullptr;
+    std::lock_guard<std::mutex> lock(g_wait_mutex);
+    if (!g_wait_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_wait_word) != cudaSuccess) return nullptr;
+        g_wait_addr[dev] = p;
+    }
+    return (unsigned long long *)g_wait_addr[dev];
+}
 
 unsigned long long *guard_word() {
 #ifdef PAVA_BOUNDS_CHECK
@@ -375,6 +395,17 @@ pava_status pava_bounds_report(unsigned long long *out3, int clear) {
     if (out3) memset(out3, 0, 3 * sizeof(unsigned long long));
     return fail(PAVA_E_UNSUPPORTED_PARAMS, "not a bounds-checked build (PAVA_BOUNDS_CHECK)");
 #endif
+}
+
+pava_status pava_wait_report(unsigned long long *out2, int clear) {
+    unsigned long long *w = pava::wait_word();
+    if (!w) return fail(PAVA_E_CUDA, "bounded-wait word unavailable");
+    unsigned long long h[2] = {0, 0};
+    PAVA_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    PAVA_CUDA(cudaMemcpy(h, w, sizeof(h), cudaMemcpyDeviceToHost), "read bounded-wait word");
+    if (clear) PAVA_CUDA(cudaMemset(w, 0, sizeof(h)), "clear bounded-wait word");
+    if (out2) memcpy(out2, h, sizeof(h));
+    return h[0] ? PAVA_E_TIMEOUT : PAVA_SUCCESS;
 }
 
 pava_status pava_set_device_memory_limit(unsigned long long bytes) {

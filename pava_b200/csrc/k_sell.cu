@@ -11,10 +11,17 @@
 // are no row-start flags, no cross-lane combine and no carries: one pass, one coalesced y
 // store per slice, no fixup launch.  Padding elements (value 0, no column) read no x.
 //
+// The SpMV stages the value and column streams through shared memory with bulk asynchronous
+// copies (cp.async.bulk, completion counted on an mbarrier): a warp keeps two pieces of its
+// slices in flight in its own shared-memory stages while it sums a third from shared memory,
+// so the bytes in flight per SM are set by shared memory (~200 KB), not by registers.
+//
 // The price is the padding, so the form is for matrices whose rows in a slice have similar
 // lengths; pava_create refuses it (PAVA_E_UNSUPPORTED_PARAMS) when padding would more than
 // double the stored elements.  No counterpart in the reference (pava's engines are CVR and
 // CSR5); it is a third engine form beside them, offered by the autotuner and the selector.
+
+#include <atomic>
 
 #include <cub/cub.cuh>
 
@@ -99,21 +106,6 @@ __global__ void sell_fill_kernel(const int *__restrict__ rp, const int *__restri
     if (lane == 0) meta[s].off = (int)off;
 }
 
-// Pipeline depth (blocks of 4 steps the value and column loads run ahead of their use) and
-// resident CTAs per SM of each value form.
-#ifndef PAVA_SELL_D64
-#define PAVA_SELL_D64 2
-#endif
-#ifndef PAVA_SELL_D32
-#define PAVA_SELL_D32 2
-#endif
-#ifndef PAVA_SELL_MINB64
-#define PAVA_SELL_MINB64 3
-#endif
-#ifndef PAVA_SELL_MINB32
-#define PAVA_SELL_MINB32 4
-#endif
-
 // Row sums.  FP64: FMA.  FP32 values and x: a product of two FP32 numbers is exact in FP64
 // (24 + 24 significant bits < 53), so the FP32 form widens both factors and sums the exact
 // products with FP64 FMAs -- an FP64 sum of exact terms, one rounding per nonzero.
@@ -131,87 +123,219 @@ template <> struct RowAcc<float> {
     __device__ __forceinline__ void reset() { s = 0.0; }
 };
 
-template <typename VT> struct SellShape;
-template <> struct SellShape<double> {
-    static constexpr int D = PAVA_SELL_D64, MINB = PAVA_SELL_MINB64;
-};
-template <> struct SellShape<float> {
-    static constexpr int D = PAVA_SELL_D32, MINB = PAVA_SELL_MINB32;
+// Bulk-copy staging.  A stage holds one piece: up to KB consecutive blocks of one slice
+// (KB = the blocks of about 3 KB of value and column stream); each warp owns STAGES stages and
+// an mbarrier per stage; CTAS_PER_SM CTAs of SELL_WARPS warps share an SM.
+constexpr int STAGE_BYTES = 3072, STAGES = 2, CTAS_PER_SM = 4;
+// Bounded waits: each try_wait may suspend the warp for up to WAIT_HINT_NS; after WAIT_TRIES
+// unsuccessful tries (about a second) the wait gives up and the kernel reports it.
+constexpr unsigned WAIT_HINT_NS = 20000;
+constexpr int WAIT_TRIES = 1 << 16;
+
+template <typename VT, typename IT> struct Stage {
+    static constexpr int BPB = 128 * (int)(sizeof(VT) + sizeof(IT));  // bytes per block
+    static constexpr int KB = STAGE_BYTES / BPB > 0 ? STAGE_BYTES / BPB : 1;
+    static constexpr int VBYTES = KB * 128 * (int)sizeof(VT), CBYTES = KB * 128 * (int)sizeof(IT);
+    static constexpr int WARP_BYTES = STAGES * (VBYTES + CBYTES) + 128;  // + barriers
+    static constexpr int CTA_BYTES = SELL_WARPS * WARP_BYTES;
+    static_assert(STAGES * 8 <= 128 && WARP_BYTES % 128 == 0, "stage layout");
 };
 
-template <bool B> struct SFlag { static constexpr bool value = B; };
+__device__ __forceinline__ void mbar_init(unsigned a) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned a, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
+                 : "memory");
+}
+// global -> this CTA's shared memory; both addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes,
+                                         unsigned mbar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity) {
+    for (int i = 0; i < WAIT_TRIES; ++i) {
+        unsigned ok;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; "
+            "selp.u32 %0, 1, 0, p; }"
+            : "=r"(ok) : "r"(a), "r"(parity), "r"(WAIT_HINT_NS) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
 
-// SpMV: one warp per slice (grid-stride over slices, persistent grid: the warps of the grid
-// work on neighbouring slices at any time, so the streams are read close to in order).  The
-// slice's blocks run through register rings of D slots: the values of block b + D and the
-// columns of block b + D + 1 are loaded while block b is summed and the x of block b + 1 is
-// gathered.  Each lane accumulates its own row; the slice ends with one coalesced store of 32
-// rows.
+// Stream blocks from a shared-memory stage (same block layout as the global streams).
+template <typename VT> __device__ __forceinline__ VBlk<VT> vblk_smem(const VT *p, int blk, int lane);
+template <> __device__ __forceinline__ VBlk<double> vblk_smem<double>(const double *p, int blk,
+                                                                      int lane) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    VBlk<double> r;
+    r.a = q[(2 * blk) * 32 + lane];
+    r.b = q[(2 * blk + 1) * 32 + lane];
+    return r;
+}
+template <> __device__ __forceinline__ VBlk<float> vblk_smem<float>(const float *p, int blk,
+                                                                    int lane) {
+    VBlk<float> r;
+    r.a = reinterpret_cast<const float4 *>(p)[blk * 32 + lane];
+    return r;
+}
+template <typename IT> __device__ __forceinline__ CBlk<IT> cblk_smem(const IT *p, int blk, int lane);
+template <> __device__ __forceinline__ CBlk<int> cblk_smem<int>(const int *p, int blk, int lane) {
+    CBlk<int> r;
+    r.a = reinterpret_cast<const int4 *>(p)[blk * 32 + lane];
+    return r;
+}
+template <> __device__ __forceinline__ CBlk<short> cblk_smem<short>(const short *p, int blk,
+                                                                    int lane) {
+    CBlk<short> r;
+    r.a = reinterpret_cast<const uint2 *>(p)[blk * 32 + lane];
+    return r;
+}
+
+// SpMV.  Warps take slices in turn (grid-stride: the warps of the grid work on neighbouring
+// slices at any time, so the streams are read close to in order).  Each warp walks its slices
+// as a sequence of pieces (<= KB blocks of one slice) with two cursors: the producer (lane 0
+// issues the bulk copies of a piece into the next free stage) runs STAGES pieces ahead of the
+// consumer, which waits for its stage's copies, sums the piece's blocks from shared memory
+// -- gathering the x of block i + 1 while block i is summed -- and hands the stage back.  A
+// slice's last piece stores its 32 rows; empty slices (no blocks) store zero rows.  A wait
+// that gives up counts itself in wait_err[0] (the first slice in wait_err[1]); the warp then
+// waits, again bounded, for the copies it still has in flight and stops.
 template <typename VT, typename IT>
-__global__ void __launch_bounds__(SELL_WARPS * 32, SellShape<VT>::MINB)
+__global__ void __launch_bounds__(SELL_WARPS * 32, CTAS_PER_SM)
 sell_spmv_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals,
                  const IT *__restrict__ cols, const VT *__restrict__ x,
                  double *__restrict__ y, long long nslices, int m, int n,
-                 unsigned long long *err) {
-    constexpr int D = SellShape<VT>::D;
-    static_assert(D >= 2 && D % 2 == 0, "the x ring of two slots needs an even depth");
+                 unsigned long long *err, unsigned long long *wait_err) {
+    using ST = Stage<VT, IT>;
+    constexpr int KB = ST::KB;
+    extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+    unsigned char *wbase = smem + w * ST::WARP_BYTES;  // [barriers | value stages | column stages]
+    const unsigned bar0 = (unsigned)__cvta_generic_to_shared(wbase);
+    const VT *sv = reinterpret_cast<const VT *>(wbase + 128);
+    const IT *sc = reinterpret_cast<const IT *>(wbase + 128 + STAGES * ST::VBYTES);
+    const unsigned sv0 = bar0 + 128, sc0 = bar0 + 128 + STAGES * ST::VBYTES;
+    if (lane == 0) {
+        for (int k = 0; k < STAGES; ++k) mbar_init(bar0 + 8 * k);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    const uint64_t pl = policy_evict_last();
     const long long nwarps = (long long)gridDim.x * SELL_WARPS;
-    for (long long s = (long long)blockIdx.x * SELL_WARPS + w; s < nslices; s += nwarps) {
-        const SellSlice S = meta[s];
-        const int NB = S.nblk;
-        const VT *vb = vals + S.off;
-        const IT *cb = cols + S.off;
-        const int xbase = sizeof(IT) == 2 ? S.colbase : 0;  // base of the 16-bit offsets
+    const long long first = (long long)blockIdx.x * SELL_WARPS + w;
+
+    // producer cursor: slice ps (with blocks), next block pb
+    long long ps = first;
+    int pb = 0;
+    SellSlice pm{0, 0, 0, 0u};
+    if (ps < nslices) pm = meta[ps];
+    while (ps < nslices && pm.nblk == 0) {
+        ps += nwarps;
+        if (ps < nslices) pm = meta[ps];
+    }
+    auto issue = [&](int k) {
+        const int len = min(KB, pm.nblk - pb);
+        const long long e0 = (long long)pm.off + (long long)pb * 128;
+        if (lane == 0) {
+            const unsigned vb = (unsigned)(len * 128 * (int)sizeof(VT));
+            const unsigned cb = (unsigned)(len * 128 * (int)sizeof(IT));
+            // the stage's last reads (generic proxy) come before the copy's writes
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(bar0 + 8 * k, vb + cb);
+            bulk_g2s(sv0 + k * ST::VBYTES, vals + e0, vb, bar0 + 8 * k);
+            bulk_g2s(sc0 + k * ST::CBYTES, cols + e0, cb, bar0 + 8 * k);
+        }
+        pb += KB;
+        if (pb >= pm.nblk) {
+            pb = 0;
+            do {
+                ps += nwarps;
+                if (ps < nslices) pm = meta[ps];
+            } while (ps < nslices && pm.nblk == 0);
+        }
+    };
+    int pending = 0;
+#pragma unroll
+    for (int k = 0; k < STAGES; ++k)
+        if (ps < nslices) { issue(k); ++pending; }
+
+    // consumer cursor: slice cs, next block cb; it writes the rows of empty slices
+    long long cs = first;
+    int cb = 0;
+    SellSlice cm{0, 0, 0, 0u};
+    auto skip_empty = [&]() {
+        while (cs < nslices) {
+            cm = meta[cs];
+            if (cm.nblk > 0) break;
+            const long long r = cs * 32 + lane;
+            if (r < m) y[r] = 0.0;
+            cs += nwarps;
+        }
+    };
+    skip_empty();
+    unsigned phases = 0;  // bit k: parity the consumer waits for on stage k
+    int k = 0;
+    RowAcc<VT> acc;
+    while (cs < nslices) {
+        if (!mbar_wait(bar0 + 8 * k, (phases >> k) & 1u)) {
+            if (lane == 0) {
+                atomicAdd(&wait_err[0], 1ull);
+                atomicCAS(&wait_err[1], 0ull, (unsigned long long)cs + 1);
+            }
+            break;
+        }
+        phases ^= 1u << k;
+        --pending;
+        const int len = min(KB, cm.nblk - cb);
+        const VT *pv = sv + k * (ST::VBYTES / (int)sizeof(VT));
+        const IT *pc = sc + k * (ST::CBYTES / (int)sizeof(IT));
+        const int xbase = sizeof(IT) == 2 ? cm.colbase : 0;  // base of the 16-bit offsets
         const VT *xb = x + xbase;
         const int xlo = -xbase, xhi = n - xbase;
-        RowAcc<VT> acc;
-        // CHK: the slice pads some rows, so each gather tests its column
-        auto walk = [&](auto chk_tag) {
-            constexpr bool CHK = decltype(chk_tag)::value;
-            auto gather4 = [&](const CBlk<IT> &cbk, VT (&xs)[4]) {
+        const bool chk = cm.flags & 1u;  // the slice pads some rows: test each column
+        auto gather4 = [&](const CBlk<IT> &cbk, VT (&xs)[4]) {
+            if (chk) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    xs[q] = CHK ? cbk.gather(q, xb, pl, xlo, xhi, err)
-                                : cbk.gather_all(q, xb, pl, xlo, xhi, err);
-            };
-            VBlk<VT> v[D];
-            CBlk<IT> c[D];
-            VT xs[2][4];
+                for (int q = 0; q < 4; ++q) xs[q] = cbk.gather(q, xb, pl, xlo, xhi, err);
+            } else {
 #pragma unroll
-            for (int j = 0; j < D; ++j) {
-                if (j < NB) {
-                    v[j] = VBlk<VT>::load(vb, j, lane, pf);
-                    c[j] = CBlk<IT>::load(cb, j, lane, pf);
-                }
-            }
-            gather4(c[0], xs[0]);
-            if (D < NB) c[0] = CBlk<IT>::load(cb, D, lane, pf);
-#pragma unroll 1
-            for (int b0 = 0; b0 < NB; b0 += D) {
-#pragma unroll
-                for (int j = 0; j < D; ++j) {  // block b = b0 + j sits in slot j
-                    const int b = b0 + j;
-                    if (b < NB) {
-                        const int jn = (j + 1) % D;  // slot of block b + 1
-                        if (b + 1 < NB) {
-                            gather4(c[jn], xs[(j + 1) & 1]);
-                            if (b + 1 + D < NB) c[jn] = CBlk<IT>::load(cb, b + 1 + D, lane, pf);
-                        }
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) acc.add(v[j].get(q), xs[j & 1][q]);
-                        if (b + D < NB) v[j] = VBlk<VT>::load(vb, b + D, lane, pf);
-                    }
-                }
+                for (int q = 0; q < 4; ++q) xs[q] = cbk.gather_all(q, xb, pl, xlo, xhi, err);
             }
         };
-        if (NB > 0) {
-            if (S.flags & 1u) walk(SFlag<true>{});
-            else walk(SFlag<false>{});
+        VT xs[2][4];
+        gather4(cblk_smem<IT>(pc, 0, lane), xs[0]);
+#pragma unroll
+        for (int i = 0; i < KB; ++i) {
+            if (i < len) {
+                if (i + 1 < len) gather4(cblk_smem<IT>(pc, i + 1, lane), xs[(i + 1) & 1]);
+                const VBlk<VT> vv = vblk_smem<VT>(pv, i, lane);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc.add(vv.get(q), xs[i & 1][q]);
+            }
         }
-        const long long r = s * 32 + lane;
-        if (r < m) y[r] = acc.value();
+        cb += KB;
+        if (cb >= cm.nblk) {  // the slice's last piece
+            const long long r = cs * 32 + lane;
+            if (r < m) y[r] = acc.value();
+            acc.reset();
+            cb = 0;
+            cs += nwarps;
+            skip_empty();
+        }
+        __syncwarp();  // every lane is done with stage k
+        if (ps < nslices) { issue(k); ++pending; }
+        k = k + 1 == STAGES ? 0 : k + 1;
+    }
+    // only after a wait gave up: let the copies still in flight land before the CTA exits
+    for (; pending > 0; --pending) {
+        mbar_wait(bar0 + 8 * k, (phases >> k) & 1u);
+        phases ^= 1u << k;
+        k = k + 1 == STAGES ? 0 : k + 1;
     }
 }
 
@@ -227,12 +351,23 @@ cudaError_t fill_t(Handle &h, const int *rp, const int *ci, const double *v, con
 
 template <typename VT, typename IT>
 cudaError_t spmv_t(const Handle &h, const void *x, void *y, cudaStream_t s) {
+    using ST = Stage<VT, IT>;
+    // more than the default 48 KB of dynamic shared memory: opted into once per device
+    static std::atomic<unsigned long long> opted{0};
+    if (h.device < 0 || h.device >= 64) return cudaErrorInvalidDevice;
+    const unsigned long long bit = 1ull << h.device;
+    if (!(opted.load() & bit)) {
+        const cudaError_t e = cudaFuncSetAttribute(
+            sell_spmv_kernel<VT, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ST::CTA_BYTES);
+        if (e != cudaSuccess) return e;
+        opted.fetch_or(bit);
+    }
     const long long want = (h.nchunks + SELL_WARPS - 1) / SELL_WARPS;
-    const long long cap = (long long)h.sm_count * SellShape<VT>::MINB;
+    const long long cap = (long long)h.sm_count * CTAS_PER_SM;
     const unsigned grid = (unsigned)(want < cap ? want : cap);
-    sell_spmv_kernel<VT, IT><<<grid, SELL_WARPS * 32, 0, s>>>(
+    sell_spmv_kernel<VT, IT><<<grid, SELL_WARPS * 32, ST::CTA_BYTES, s>>>(
         (const SellSlice *)h.meta, (const VT *)h.vals, (const IT *)h.cols, (const VT *)x,
-        (double *)y, h.nchunks, h.m, h.n, guard_word());
+        (double *)y, h.nchunks, h.m, h.n, guard_word(), wait_word());
     return cudaGetLastError();
 }
 

@@ -80,6 +80,10 @@ void set_last_error(const std::string &msg);
 // builds with PAVA_BOUNDS_CHECK; nullptr in ordinary builds, whose kernels never test it.
 unsigned long long *guard_word();
 
+// Device address of the bounded-wait word (two 64-bit words: waits that gave up, and the first
+// one's site + 1) on the current device; in every build.  nullptr when it cannot be resolved.
+unsigned long long *wait_word();
+
 // CSR5 tiles per chunk.  The persistent grid keeps `warps` warps resident (24 per SM); each
 // takes chunks in turn, so a chunk count just above a multiple of `warps` leaves a last wave
 // that few warps run.

@@ -41,6 +41,21 @@ def _bounds_report(request):
                          f"{out[1]} with index {out[2]}")
 
 
+@pytest.fixture(autouse=True)
+def _wait_report(request):
+    """Every GPU test must leave the bounded-wait word at zero: no kernel gave up waiting on
+    its bulk copies (a wait that gives up ends the kernel early with wrong rows)."""
+    yield
+    if "cuda" not in request.fixturenames:
+        return
+    import ctypes
+    from pava_b200 import _abi
+    out = (ctypes.c_ulonglong * 2)()
+    st = _abi.gpu().pava_wait_report(out, 1)
+    assert st == 0 and out[0] == 0, (f"{out[0]} bounded waits gave up, the first at site "
+                                      f"{out[1]}")
+
+
 @pytest.fixture(scope="session")
 def cuda():
     import torch
