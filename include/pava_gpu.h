@@ -310,7 +310,7 @@ pava_status pava_free_device_csr(pava_csr *A);
 /* ---- Learned form selector ----------------------------------------------------------
  * No counterpart in the reference (which runs every format it is asked for; its only tile
  * knob is CSR5's sigma, anonymouslibHandle::setSigma, csr5/anonymouslib_avx512.h:265).
- * The selector chooses among PAVA_NVARIANTS = 30 engine forms: a kernel variant and its tile
+ * The selector chooses among PAVA_NVARIANTS = 32 engine forms: a kernel variant and its tile
  * parameters, the same set pava_autotune searches for one right-hand side:
  *    0 ..  3  CVR, steps 64 / 128, each with 32-bit columns and with PAVA_INDEX_AUTO
  *             (v = 2 * (steps == 128) + auto)
@@ -319,20 +319,24 @@ pava_status pava_free_device_csr(pava_csr *A);
  *             (v = 4 + 4 * (sigma == 32) + 2 * wave + auto)
  *   12 .. 29  plain CSR row groups, lanes per row 1, 2, 4, 8, 16, 32, with 1, 4 or 16 row
  *             groups per warp tile (v = 12 + 3 * log2(lanes) + {0, 1, 2})
- * Forms fall into PAVA_NFAMILIES = 6 kernel variants (pava_variant_family): CVR 64, CVR 128,
- * CSR5 16, CSR5 32, CSR with <= 4 lanes per row, CSR with >= 8.  A matrix is described by 12
- * structural features (pava_features); an MLP 12-64-64-30 predicts the log-time of every form
- * (so also each variant's best time, the minimum over its forms) and the smallest prediction
- * wins.  The network is trained on the GPU by the library's own forward / backward / Adam
- * kernels on timings that pava_time_variants measures; exhaustive timing of all 30 forms is
- * both the fallback and the yardstick of the selector's regret. */
-#define PAVA_NVARIANTS 30
-#define PAVA_NFAMILIES 6
+ *   30 .. 31  SELL, 32-bit columns or PAVA_INDEX_AUTO (v = 30 + auto); refused by matrices
+ *             whose slice padding would more than double the stored elements
+ * Forms fall into PAVA_NFAMILIES = 7 kernel variants (pava_variant_family): CVR 64, CVR 128,
+ * CSR5 16, CSR5 32, CSR with <= 4 lanes per row, CSR with >= 8, SELL.  A matrix is described
+ * by 12 structural features (pava_features); an MLP 12-64-64-32 predicts the log-time of every
+ * form (so also each variant's best time, the minimum over its forms) and the smallest
+ * prediction among the forms that take the matrix wins (pava_create_selected moves to the
+ * next prediction when a form refuses it).  The network is trained on the GPU by the
+ * library's own forward / backward / Adam kernels on timings that pava_time_variants
+ * measures; exhaustive timing of all 32 forms is both the fallback and the yardstick of the
+ * selector's regret. */
+#define PAVA_NVARIANTS 32
+#define PAVA_NFAMILIES 7
 #define PAVA_TILES_WAVE (-1) /* pava_opts.tiles_per_chunk: the wave-balanced count for A */
 #define PAVA_MLP_IN 12
 #define PAVA_MLP_HIDDEN 64
-#define PAVA_MLP_OUT 30
-#define PAVA_MLP_NPARAM 6942
+#define PAVA_MLP_OUT 32
+#define PAVA_MLP_NPARAM 7072
 /* Form v's format and options (options zeroed except the form's tile parameters). */
 pava_status pava_variant(int v, int *format, pava_opts *opts);
 /* The kernel variant (0 .. PAVA_NFAMILIES - 1) form v belongs to, or -1 if v is out of range. */
@@ -344,7 +348,7 @@ int pava_variant_family(int v);
  *   9 share of nonzeros within 64 of the diagonal   10 distinct 128-byte x lines per
  *   nonzero   11 log10(mean row span / n + 1e-7).  Integer accumulation: same bits each run. */
 pava_status pava_features(const pava_csr *A, float *out12, void *stream);
-/* Converts A into each of the 30 forms and times its SpMV (two warm-ups, median of `reps`
+/* Converts A into each of the 32 forms and times its SpMV (two warm-ups, median of `reps`
  * CUDA-event timings, x and y on the device): pava_autotune for k = 1, in form order.
  * ms[v] < 0 when form v failed; a wave-balanced CSR5 form whose tile count equals the default
  * one is the same form and gets its twin's time; *best = fastest. */
@@ -352,17 +356,17 @@ pava_status pava_time_variants(const pava_csr *A, int reps, double *ms, int *bes
 typedef struct pava_mlp pava_mlp;
 /* A network with He-uniform weights from `seed`, zero biases, identity normalisation. */
 pava_status pava_mlp_create(uint64_t seed, pava_mlp **out);
-/* Parameters (PAVA_MLP_NPARAM floats: W1[64][12] b1 W2[64][64] b2 W3[30][64] b3) and the
+/* Parameters (PAVA_MLP_NPARAM floats: W1[64][12] b1 W2[64][64] b2 W3[32][64] b3) and the
  * feature normalisation (x - mean) / std applied to every batch; any pointer may be NULL.
  * Setting parameters resets the Adam state. */
 pava_status pava_mlp_get_params(const pava_mlp *m, float *params, float *mean12, float *std12);
 pava_status pava_mlp_set_params(pava_mlp *m, const float *params, const float *mean12,
                                 const float *std12);
-/* Uploads a batch: B x 12 raw features, optional B x 30 targets and 0/1 mask (NULL mask = all
+/* Uploads a batch: B x 12 raw features, optional B x 32 targets and 0/1 mask (NULL mask = all
  * ones).  The loss is the masked mean squared error. */
 pava_status pava_mlp_set_batch(pava_mlp *m, int B, const float *X, const float *T,
                                const float *mask);
-/* Outputs for the current batch (B x 30, host). */
+/* Outputs for the current batch (B x 32, host). */
 pava_status pava_mlp_forward(pava_mlp *m, float *Y);
 /* Gradient of the loss w.r.t. the parameters (PAVA_MLP_NPARAM floats, host) and the loss. */
 pava_status pava_mlp_gradient(pava_mlp *m, float *grad, float *loss);

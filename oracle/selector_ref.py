@@ -7,14 +7,14 @@ for the CUDA kernels.
 
 * ``features(rp, ci, n)``  -- the 12 structural features of pava_features (float64 here;
   the kernel accumulates the same integer statistics, so they agree to float32 rounding)
-* ``mlp_forward`` / ``mlp_loss_grad`` -- the MLP 12-64-64-30 with ReLU and the masked mean
+* ``mlp_forward`` / ``mlp_loss_grad`` -- the MLP 12-64-64-32 with ReLU and the masked mean
   squared error, forward and backward in float64, for the gradient check of pava_mlp_gradient
 """
 from __future__ import annotations
 
 import numpy as np
 
-IN, HID, OUT = 12, 64, 30
+IN, HID, OUT = 12, 64, 32
 OW1, OB1 = 0, HID * IN
 OW2, OB2 = OB1 + HID, OB1 + HID + HID * HID
 OW3, OB3 = OB2 + HID, OB2 + HID + OUT * HID

@@ -75,7 +75,7 @@ class PavaGenParams(ctypes.Structure):
 
 
 GEN_STENCIL, GEN_BANDED, GEN_POWERLAW, GEN_BLOCKDIAG = 0, 1, 2, 3
-NVARIANTS, NFAMILIES, MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_NPARAM = 30, 6, 12, 64, 30, 6942
+NVARIANTS, NFAMILIES, MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_NPARAM = 32, 7, 12, 64, 32, 7072
 TILES_WAVE = -1
 
 

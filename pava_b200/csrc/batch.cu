@@ -173,7 +173,7 @@ pava_status build_union(int count, const pava_csr *mats, cudaStream_t s, pava_ba
     return PAVA_SUCCESS;
 }
 
-// Built-in candidate forms for k right-hand sides: for k = 1 the 30 forms of pava_variant in
+// Built-in candidate forms for k right-hand sides: for k = 1 the 32 forms of pava_variant in
 // their order (the selector's space); for k > 1 the row-group shapes (at most 72 for k <= 128).
 std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
     std::vector<std::pair<int, pava_opts>> c;

@@ -1,7 +1,8 @@
-// The 30 engine forms the learned selector chooses between (a kernel variant and its tile
+// The 32 engine forms the learned selector chooses between (a kernel variant and its tile
 // parameters: the k = 1 candidate set of pava_autotune), their exhaustive timing, and
 // selection: features (k_features.cu) -> MLP (k_mlp.cu) -> the form with the smallest
-// predicted log-time.  With no trained network, selection falls back to timing all 30.
+// predicted log-time that takes the matrix.  With no trained network, selection falls back to
+// timing all 32.
 
 #include <string.h>
 
@@ -28,12 +29,15 @@ bool form_of(int v, int &format, pava_opts &o) {
         o.sigma = (q & 4) ? 32 : 16;
         o.tiles_per_chunk = (q & 2) ? PAVA_TILES_WAVE : 0;
         o.index_mode = (q & 1) ? PAVA_INDEX_AUTO : PAVA_INDEX_I32;
-    } else {
+    } else if (v < 30) {
         const int q = v - 12;
         static const int groups[3] = {1, 4, 16};
         format = PAVA_FORMAT_CSR;
         o.lanes_per_row = 1 << (q / 3);
         o.rows_per_tile = groups[q % 3] * (32 / o.lanes_per_row);
+    } else {
+        format = PAVA_FORMAT_SELL;
+        o.index_mode = (v & 1) ? PAVA_INDEX_AUTO : PAVA_INDEX_I32;
     }
     return true;
 }
@@ -55,7 +59,8 @@ int pava_variant_family(int v) {
     if (v < 0 || v >= PAVA_NVARIANTS) return -1;
     if (v < 4) return v < 2 ? 0 : 1;
     if (v < 12) return v < 8 ? 2 : 3;
-    return (v - 12) / 3 <= 2 ? 4 : 5;  // lanes per row <= 4 / >= 8
+    if (v < 30) return (v - 12) / 3 <= 2 ? 4 : 5;  // lanes per row <= 4 / >= 8
+    return 6;
 }
 
 pava_status pava_time_variants(const pava_csr *A, int reps, double *ms, int *best) {
@@ -93,18 +98,31 @@ pava_status pava_create_selected(const pava_csr *A, pava_mlp *m, void *stream,
     *out = nullptr;
     int v = -1;
     pava_status st;
+    float pred[PAVA_MLP_OUT];
     if (m && A->on_device) {
-        st = pava_select(m, A, &v, nullptr);
-    } else {  // no network (or a host CSR): exhaustive timing of the 30 forms
+        st = pava_select(m, A, &v, pred);
+    } else {  // no network (or a host CSR): exhaustive timing of the 32 forms
         double ms[PAVA_NVARIANTS];
         st = pava_time_variants(A, 3, ms, &v);
+        for (int u = 0; u < PAVA_NVARIANTS; ++u) pred[u] = ms[u] > 0 ? (float)ms[u] : 3e38f;
     }
     if (st != PAVA_SUCCESS) return st;
-    int fmt;
-    pava_opts o;
-    pava_variant(v, &fmt, &o);
-    st = pava_create(A, fmt, &o, stream, out);
-    if (st == PAVA_SUCCESS && variant) *variant = v;
+    // the forms in order of prediction; a form that refuses the matrix (SELL padding) passes
+    // the choice on to the next
+    std::vector<int> order(PAVA_NVARIANTS);
+    for (int u = 0; u < PAVA_NVARIANTS; ++u) order[u] = u;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pred[a] < pred[b]; });
+    for (int u : order) {
+        int fmt;
+        pava_opts o;
+        pava_variant(u, &fmt, &o);
+        st = pava_create(A, fmt, &o, stream, out);
+        if (st == PAVA_SUCCESS) {
+            if (variant) *variant = u;
+            return st;
+        }
+        if (st != PAVA_E_UNSUPPORTED_PARAMS) return st;
+    }
     return st;
 }
 

@@ -9,16 +9,18 @@ lognormal power-law and block-diagonal (dense blocks of 8..64); rows log-uniform
 [10^4, 10^7] and nonzeros log-uniform in [10^5, 10^8] (each family's row length follows
 from the pair, within its own range); values N(0,1), FP64.  Every matrix is generated on the
 GPU (pava_gen_device), described by its 12 structural features (pava_features), and each of
-the 30 engine forms -- six kernel variants with their tile parameters, the k = 1 candidate
+the 32 engine forms -- seven kernel variants with their tile parameters, the k = 1 candidate
 set of pava_autotune -- is converted and timed on it (pava_time_variants: median of 5
 CUDA-event timings after two warm-ups, x and y resident).  The file keeps the features, the
 times and each matrix's family, rows and nonzeros.
 
-Network: MLP 12-64-64-30 (ReLU, FP32), trained on the GPU by the library's own kernels
+Network: MLP 12-64-64-32 (ReLU, FP32), trained on the GPU by the library's own kernels
 (pava_mlp_train: full-batch Adam on the masked mean squared error of standardised
-log-times).  Selection = the form with the smallest predicted log-time; a kernel variant's
-predicted time is the smallest over its forms.  Regret of a choice = t_chosen / t_best - 1,
-t_best from the exhaustive timing of all 30 forms (the full autotune).
+log-times).  Selection = the form with the smallest predicted log-time among the forms that
+take the matrix (a SELL form refuses a matrix whose slice padding would more than double it,
+and pava_create_selected then moves to the next prediction); a kernel variant's predicted
+time is the smallest over its forms.  Regret of a choice = t_chosen / t_best - 1, t_best
+from the exhaustive timing of all 32 forms (the full autotune).
 """
 from __future__ import annotations
 
@@ -32,7 +34,7 @@ import numpy as np
 from . import _abi
 
 FAMILIES = ["stencil", "banded", "powerlaw", "blockdiag"]
-FAMILY_NAMES = ["cvr_s64", "cvr_s128", "csr5_s16", "csr5_s32", "csr_l1_4", "csr_l8_32"]
+FAMILY_NAMES = ["cvr_s64", "cvr_s128", "csr5_s16", "csr5_s32", "csr_l1_4", "csr_l8_32", "sell"]
 
 
 def _form_names():
@@ -47,15 +49,17 @@ def _form_names():
     for gl in (1, 2, 4, 8, 16, 32):
         for g in (1, 4, 16):
             out.append(f"csr_l{gl}_g{g}")
+    out += ["sell_i32", "sell_auto"]
     return out
 
 
 FORM_NAMES = _form_names()
 # the kernel variant each form belongs to (pava_variant_family)
-FORM_FAMILY = np.array([0, 0, 1, 1] + [2] * 4 + [3] * 4 + [4] * 9 + [5] * 9)
+FORM_FAMILY = np.array([0, 0, 1, 1] + [2] * 4 + [3] * 4 + [4] * 9 + [5] * 9 + [6] * 2)
 # each variant's default form, the one a selector of the kernel variant alone would run (CVR /
-# CSR5 with default tiles and 32-bit columns, CSR 4 and 32 lanes with 4 row groups per tile)
-FAMILY_DEFAULT_FORM = np.array([0, 2, 4, 8, 12 + 3 * 2 + 1, 12 + 3 * 5 + 1])
+# CSR5 / SELL with default tiles and 32-bit columns, CSR 4 and 32 lanes with 4 row groups per
+# tile)
+FAMILY_DEFAULT_FORM = np.array([0, 2, 4, 8, 12 + 3 * 2 + 1, 12 + 3 * 5 + 1, 30])
 N_TRAIN, N_TEST = 2000, 200
 
 
@@ -235,6 +239,13 @@ def regret(times_ms, choice):
     return chosen / best - 1.0
 
 
+def choose(pred, times_ms):
+    """The selection rule of pava_create_selected: the smallest prediction among the forms that
+    take the matrix (a form that refused it has no time; its refusal costs one conversion
+    attempt, which regret does not count)."""
+    return np.where(times_ms > 0, pred, np.inf).argmin(1)
+
+
 def train_selector(data, epochs=3000, lr=3e-3, seed=0):
     """Trains on the first n_train matrices; returns the network and a report on the held-out
     ones (selector regret, the regret of the best single fixed variant, and of a row-length
@@ -255,7 +266,7 @@ def train_selector(data, epochs=3000, lr=3e-3, seed=0):
     hist = net.train(epochs, lr)
     pred_tr = net.forward(Ftr)
     pred = net.forward(Fte)
-    choice = pred.argmin(1)
+    choice = choose(pred, Tms[ntr:])
     reg = regret(Tms[ntr:], choice)
     # without the network: the one variant that is best on average over the training set
     tr_reg = np.stack([regret(Tms[:ntr], np.full(ntr, v)) for v in range(_abi.NVARIANTS)])
@@ -265,10 +276,11 @@ def train_selector(data, epochs=3000, lr=3e-3, seed=0):
     # parameters: what predicting the tile parameters adds
     fam_pred = np.stack([np.where(FORM_FAMILY == f, pred, np.inf).min(1)
                          for f in range(_abi.NFAMILIES)], 1)
+    fam_pred = np.where(Tms[ntr:][:, FAMILY_DEFAULT_FORM] > 0, fam_pred, np.inf)
     reg_family = regret(Tms[ntr:], FAMILY_DEFAULT_FORM[fam_pred.argmin(1)])
     report = {
         "train_loss_first": float(hist[0]), "train_loss_last": float(hist[-1]),
-        "train_regret_mean": float(regret(Tms[:ntr], pred_tr.argmin(1)).mean()),
+        "train_regret_mean": float(regret(Tms[:ntr], choose(pred_tr, Tms[:ntr])).mean()),
         "heldout": len(Fte),
         "selector_regret_mean": float(reg.mean()),
         "selector_regret_median": float(np.median(reg)),

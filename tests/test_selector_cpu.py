@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from oracle import selector_ref as R
+from pava_b200 import _abi
 from pava_b200 import selector as S
 
 DATA = os.path.join(os.path.dirname(__file__), "golden", "selector", "selector_timings.npz")
@@ -17,9 +18,13 @@ def test_training_set_file():
     d = np.load(DATA)
     n = int(d["n_train"]) + int(d["n_test"])
     assert (int(d["n_train"]), int(d["n_test"])) == (2000, 200)
-    assert d["features"].shape == (n, 12) and d["times_ms"].shape == (n, 30)
+    assert d["features"].shape == (n, 12) and d["times_ms"].shape == (n, _abi.NVARIANTS)
     assert np.isfinite(d["features"]).all()
-    assert (d["times_ms"] > 0).mean() > 0.99          # nearly every variant ran
+    sell = S.FORM_FAMILY == 6
+    assert (d["times_ms"][:, ~sell] > 0).mean() > 0.99  # nearly every other form ran
+    # SELL takes the stencils and banded matrices and refuses the heavy-tailed power laws
+    took = (d["times_ms"][:, sell] > 0).all(1)
+    assert took[d["family"] == 0].mean() > 0.9 and took[d["family"] == 2].mean() < 0.5
     assert np.all(np.bincount(d["family"], minlength=4) == n // 4)
     assert d["rows"].min() >= 1e4 - 1 and d["rows"].max() <= 1e7
     assert d["nnz"].min() >= 5e4 and d["nnz"].max() <= 1.1e8
@@ -77,7 +82,7 @@ def test_cpu_features_small():
 
 
 def test_form_space_matches_the_library():
-    """The 30 forms: pava_variant's formats and tile parameters, their kernel variant
+    """The 32 forms: pava_variant's formats and tile parameters, their kernel variant
     (pava_variant_family), and the names and families the selector reports use."""
     import ctypes
     from pava_b200 import _abi
@@ -97,6 +102,8 @@ def test_form_space_matches_the_library():
             w = "tiles_wave" if o.tiles_per_chunk == _abi.TILES_WAVE else "tiles_default"
             assert o.tiles_per_chunk in (0, _abi.TILES_WAVE)
             assert name == f"csr5_s{o.sigma}_{w}_{idx}"
+        elif f.value == _abi.FORMAT_SELL:
+            assert name == f"sell_{idx}"
         else:
             assert f.value == _abi.FORMAT_CSR
             groups = o.rows_per_tile // (32 // o.lanes_per_row)
@@ -105,7 +112,7 @@ def test_form_space_matches_the_library():
                o.rows_per_tile)
         assert key not in seen
         seen.add(key)
-    assert L.pava_variant(30, None, None) == _abi.E_INVALID_ARG
+    assert L.pava_variant(_abi.NVARIANTS, None, None) == _abi.E_INVALID_ARG
     assert L.pava_variant_family(-1) == -1
     for fam, v in enumerate(S.FAMILY_DEFAULT_FORM):
         assert S.FORM_FAMILY[v] == fam
