@@ -235,12 +235,19 @@ def test_autotune_k1_runs_every_candidate(cuda):
     A = M.powerlaw(100_000, mean=16.0, cap=20_000, seed=27)
     ents, best = autotune(A, k=1, reps=3)
     forms = {e["format"] for e in ents}
-    assert {"cvr", "csr5", "csr"} <= forms
-    # CVR / CSR5 come with 32-bit columns and with 16-bit offsets where they reach
+    assert {"cvr", "csr5", "csr", "sell"} <= forms
+    # CVR / CSR5 / SELL come with 32-bit columns and with 16-bit offsets where they reach
     modes = {(e["format"], e["opts"]["index_mode"]) for e in ents if e["format"] != "csr"}
-    assert modes == {(f, m) for f in ("cvr", "csr5") for m in (_abi.INDEX_I32, _abi.INDEX_AUTO)}
-    assert all(e["ms"] > 0 and e["status"] == 0 for e in ents)
-    assert ents[best]["ms"] == min(e["ms"] for e in ents)
+    assert modes == {(f, m) for f in ("cvr", "csr5", "sell")
+                     for m in (_abi.INDEX_I32, _abi.INDEX_AUTO)}
+    # SELL refuses the power-law rows (its padding would be ~10x); every other form runs
+    assert not M.sell_accepts(A)
+    for e in ents:
+        if e["format"] == "sell":
+            assert e["status"] == _abi.E_UNSUPPORTED_PARAMS and e["ms"] < 0
+        else:
+            assert e["ms"] > 0 and e["status"] == 0
+    assert ents[best]["ms"] == min(e["ms"] for e in ents if e["ms"] > 0)
     # the winner computes the right product
     torch = cuda
     x = M.uniform(A.n, seed=28)
