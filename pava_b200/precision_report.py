@@ -1,5 +1,6 @@
-"""FP32C error report: per matrix, the relative error per row of the FP32-compensated forms
-(FP32 values and x, compensated FP32 accumulation, FP64 carries and y) against the FP64 form.
+"""FP32C error report: per matrix, the relative error per row of the FP32C forms (FP32 values
+and x, FP64 y; CSR5 and CVR: compensated FP32 accumulation with FP64 carries; SELL, where it
+takes the matrix: the exact products summed in FP64) against the FP64 form.
 
     python -m pava_b200.precision_report            # all matrices, full size
     python -m pava_b200.precision_report --only c3
@@ -8,7 +9,7 @@ Two errors per matrix and FP32C form, each as max and mean over rows of
 |y - y_ref| / max(|y_ref|, sum_j |a_ij x_j|) (cancellation-aware denominator):
 
 * arithmetic -- against the FP64 form run on the same FP32-rounded values and x: the error of
-  the compensated FP32 arithmetic alone (the bound the FP32C form is held to is 1e-9);
+  the FP32C arithmetic alone (the bound the FP32C form is held to is 1e-9);
 * total -- against the FP64 form on the original FP64 values and x: adds the rounding of the
   inputs to FP32 when they are not FP32-representable (about 1e-7 relative).
 
@@ -29,7 +30,7 @@ from . import _abi
 from . import matrices as M
 from .api import SpMatrix
 
-FORMS32 = [("csr5", dict(sigma=32)), ("cvr", dict(steps=128))]
+FORMS32 = [("csr5", dict(sigma=32)), ("cvr", dict(steps=128)), ("sell", dict())]
 
 
 def make(name):
@@ -75,6 +76,8 @@ def report(torch, name):
     abr = absum_of(Ar, xr)
     x32 = xd.float()
     for fmt, kw in FORMS32:
+        if fmt == "sell" and not M.sell_accepts(A):
+            continue  # SELL refuses the matrix (padding)
         mat = SpMatrix(A, fmt, precision=_abi.PREC_FP32C, index_mode=_abi.INDEX_AUTO, **kw)
         y32 = mat.spmv(x32).cpu().numpy()
         im = mat.info()["index_mode"]
