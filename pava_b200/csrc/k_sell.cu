@@ -22,6 +22,7 @@
 // CSR5); it is a third engine form beside them, offered by the autotuner and the selector.
 
 #include <atomic>
+#include <climits>
 
 #include <cub/cub.cuh>
 
@@ -61,6 +62,12 @@ __global__ void sell_plan_kernel(const int *__restrict__ rp, const int *__restri
     }
     const int nblk = (mx + 3) / 4;
     const bool pads = __any_sync(FULL, len < 4 * nblk);
+    int mn = len;  // the shortest row: blocks before mn / 4 hold no padding
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const int t = __shfl_xor_sync(FULL, mn, o);
+        mn = t < mn ? t : mn;
+    }
     int cmin = 0x7fffffff, cmax = -1;
     if (want_base) {
         for (int j = 0; j < len; ++j) {
@@ -79,7 +86,7 @@ __global__ void sell_plan_kernel(const int *__restrict__ rp, const int *__restri
         meta[s].off = 0;
         meta[s].nblk = nblk;
         meta[s].colbase = cmax >= 0 ? (int)(((long long)cmin + cmax) / 2) : 0;
-        meta[s].flags = pads ? 1u : 0u;
+        meta[s].flags = pads ? 1u | ((unsigned)(mn / 4) << 1) : 0u;
         nblk_out[s] = nblk;
     }
 }
@@ -297,9 +304,10 @@ sell_spmv_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
         const int xbase = sizeof(IT) == 2 ? cm.colbase : 0;  // base of the 16-bit offsets
         const VT *xb = x + xbase;
         const int xlo = -xbase, xhi = n - xbase;
-        const bool chk = cm.flags & 1u;  // the slice pads some rows: test each column
-        auto gather4 = [&](const CBlk<IT> &cbk, VT (&xs)[4]) {
-            if (chk) {
+        // blocks from pad_from on hold padding: their gathers test each column
+        const int pad_from = (cm.flags & 1u) ? (int)(cm.flags >> 1) - cb : INT_MAX;
+        auto gather4 = [&](const CBlk<IT> &cbk, VT (&xs)[4], int i) {
+            if (i >= pad_from) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) xs[q] = cbk.gather(q, xb, pl, xlo, xhi, err);
             } else {
@@ -308,11 +316,11 @@ sell_spmv_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
             }
         };
         VT xs[2][4];
-        gather4(cblk_smem<IT>(pc, 0, lane), xs[0]);
+        gather4(cblk_smem<IT>(pc, 0, lane), xs[0], 0);
 #pragma unroll
         for (int i = 0; i < KB; ++i) {
             if (i < len) {
-                if (i + 1 < len) gather4(cblk_smem<IT>(pc, i + 1, lane), xs[(i + 1) & 1]);
+                if (i + 1 < len) gather4(cblk_smem<IT>(pc, i + 1, lane), xs[(i + 1) & 1], i + 1);
                 const VBlk<VT> vv = vblk_smem<VT>(pv, i, lane);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) acc.add(vv.get(q), xs[i & 1][q]);

@@ -33,7 +33,8 @@ struct SellSlice {
     int off;         // first element of the slice in the value and column streams
     int nblk;        // 4-step blocks: the slice's longest row, rounded up to 4, over 4
     int colbase;     // DELTA16: base column of the 16-bit offsets
-    unsigned flags;  // bit 0: some row of the slice is padded (padding reads no x)
+    unsigned flags;  // bit 0: some row of the slice is padded (padding reads no x); bits 1..31:
+                     // the first block holding padding (the shortest row / 4)
 };
 static_assert(sizeof(SellSlice) == 16, "SellSlice layout");
 

@@ -122,7 +122,8 @@ def test_sell_padding_threshold(cuda):
 def test_sell_empty_rows_ignore_nonfinite_x(cuda):
     """Padding and empty rows read no x: x is non-finite where no element reads it, and every
     row comes out finite, the empty ones exactly 0."""
-    A = _from_lengths([0, 3, 0, 5, 1, 0] * 11, 500, 15)
+    A = _from_lengths([0, 4, 0, 4, 3, 0, 4, 2] * 8, 500, 15)
+    assert M.sell_accepts(A)
     read = np.zeros(A.n, bool)
     read[A.ci] = True
     x = M.uniform(A.n, seed=16)
