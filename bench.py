@@ -13,8 +13,10 @@ steps as it does in any SpMV loop.
 
 Under torchrun (N > 1) every rank runs its own replica (the path has no exchange step);
 time is the max over ranks and value the aggregate of all ranks.  At N = 1 the line also
-carries `precision_form`: FP64 against the FP32-compensated form on the 128^3 27-point
-stencil (speed-up and error), measured after the timed region (--no-precision skips it).
+carries, measured after the timed region: `precision_form`, FP64 against the FP32C form on the
+128^3 27-point stencil (speed-up and error; --no-precision skips it); `batch_form`, the
+4,096-matrix batching workload (--no-batch); and `small_form`, the 512^2 Laplacian and the
+banded matrix with L2 flushed before every SpMV (--no-small).
 """
 from __future__ import annotations
 
@@ -53,6 +55,8 @@ def parse():
                    help="skip the batching measurement (4,096-matrix union, k = 1 and 8)")
     p.add_argument("--no-precision", action="store_true",
                    help="skip the FP64 vs FP32C comparison on the 27-point stencil")
+    p.add_argument("--no-small", action="store_true",
+                   help="skip the 512^2 Laplacian / banded measurement")
     p.add_argument("--variants", default="cvr:steps=64,cvr:steps=128,csr5:sigma=16,csr5:sigma=32",
                    help="FP64 candidates for the chosen variant")
     return p.parse_args()
@@ -445,6 +449,8 @@ def main():
             line["precision_form"] = precision_form(torch, stream)
         if world == 1 and not args.no_batch:
             line["batch_form"] = batch_form(torch)
+        if world == 1 and not args.no_small:
+            line["small_form"] = small_form(torch, stream, peak)
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -500,6 +506,53 @@ def batch_form(torch, count=4096, reps=10):
                             "replay_equals_launch": bool(torch.equal(y, direct))}
             b.close()
         out.update({"rows": b.m, "nnz": b.nnz})
+        return out
+    except Exception as e:  # a side measurement; the headline line stands without it
+        return {"unavailable": f"failed: {e}"}
+
+
+def small_form(torch, stream, peak, reps=15):
+    """FP64 SpMV on two more of the benchmark's matrices, each SpMV timed alone with L2 flushed
+    first (a 256 MB write between reps; CUDA events on the stream, median of `reps` after 3
+    warm-ups): the 512^2 5-point Laplacian (262,144 rows, 1,308,672 nnz, 21 MB: launch- and
+    latency-bound) and the banded matrix (1,048,576 rows, half-bandwidth 64, 24 per row).
+    Forms: CSR5 sigma 16, CVR steps 32, SELL with 32-bit columns and with 16-bit offsets; the
+    fastest is reported with its GB/s (compulsory bytes, 12 per nonzero) and fraction of the
+    copy bandwidth."""
+    from pava_b200 import _abi
+    from pava_b200 import matrices as M
+    from pava_b200.api import SpMatrix
+    try:
+        sp = stream.cuda_stream
+        flush = torch.empty(32 << 20, dtype=torch.float64, device="cuda")
+        out = {}
+        for key, A in (("laplace512", M.laplace2d(512)), ("banded", M.banded(1_048_576, 64, 24))):
+            x = torch.from_numpy(M.uniform(A.n, seed=5)).cuda()
+            y = torch.empty(A.m, dtype=torch.float64, device="cuda")
+            alg = A.nnz * 12.0 + 4.0 * (A.m + 1) + 8.0 * A.n + 8.0 * A.m
+            forms = {}
+            for fmt, kw in (("csr5", dict(sigma=16)), ("cvr", dict(steps=32)), ("sell", {}),
+                            ("sell", dict(index_mode=_abi.INDEX_DELTA16))):
+                mat = SpMatrix(A, fmt, **kw)
+                ts = []
+                with torch.cuda.stream(stream):
+                    for r in range(reps + 3):
+                        flush.fill_(float(r))
+                        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        a.record(stream)
+                        mat.spmv_raw(x.data_ptr(), y.data_ptr(), sp, 0)
+                        b.record(stream)
+                        b.synchronize()
+                        if r >= 3:
+                            ts.append(a.elapsed_time(b))
+                mat.close()
+                forms[fmt + "".join(f"_{k}{v}" for k, v in kw.items())] = float(np.median(ts))
+            best = min(forms, key=forms.get)
+            gbs = alg / (forms[best] * 1e-3) / 1e9
+            out[key] = {"rows": A.m, "nnz": A.nnz, "form": best, "ms": round(forms[best], 5),
+                        "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4),
+                        "forms_ms": {k: round(v, 5) for k, v in forms.items()}}
+        out["l2"] = "flushed before every SpMV (256 MB write)"
         return out
     except Exception as e:  # a side measurement; the headline line stands without it
         return {"unavailable": f"failed: {e}"}
