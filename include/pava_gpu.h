@@ -374,11 +374,13 @@ pava_status pava_mlp_gradient(pava_mlp *m, float *grad, float *loss);
  * loss_hist (may be NULL) receives the loss before each step. */
 pava_status pava_mlp_train(pava_mlp *m, int epochs, float lr, float *loss_hist);
 pava_status pava_mlp_destroy(pava_mlp *m);
-/* The form the network predicts fastest for a device CSR (and the 30 predictions).  Uses
- * the network's batch slot (a 1-sample batch replaces the current one). */
-pava_status pava_select(pava_mlp *m, const pava_csr *A, int *variant, float *pred30);
+/* The form the network predicts fastest for a device CSR (and the 32 predictions), whether
+ * or not that form takes the matrix.  Uses the network's batch slot (a 1-sample batch
+ * replaces the current one). */
+pava_status pava_select(pava_mlp *m, const pava_csr *A, int *variant, float *pred32);
 /* pava_create with the selected form: by the network when m != NULL and A is on the
- * device, otherwise by timing all 30 (the exhaustive fallback). */
+ * device (the predictions in order, past any form that refuses the matrix), otherwise by
+ * timing all 32 (the exhaustive fallback). */
 pava_status pava_create_selected(const pava_csr *A, pava_mlp *m, void *stream,
                                  pava_handle **out, int *variant);
 

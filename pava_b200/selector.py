@@ -156,7 +156,7 @@ def build_dataset(n_train=N_TRAIN, n_test=N_TEST, reps=5, log_every=100):
 # ---- network ------------------------------------------------------------------------------
 
 class Network:
-    """pava_mlp: the MLP 12-64-64-6 living on the GPU."""
+    """pava_mlp: the MLP 12-64-64-32 living on the GPU."""
 
     def __init__(self, seed: int = 0):
         h = _abi.c_void_p()
