@@ -26,6 +26,7 @@
 
 #include <cub/cub.cuh>
 
+#include "k_bulk.cuh"
 #include "k_stream.cuh"
 #include "pava_internal.h"
 
@@ -134,11 +135,6 @@ template <> struct RowAcc<float> {
 // (KB = the blocks of about 3 KB of value and column stream); each warp owns STAGES stages and
 // an mbarrier per stage; CTAS_PER_SM CTAs of SELL_WARPS warps share an SM.
 constexpr int STAGE_BYTES = 3072, STAGES = 2, CTAS_PER_SM = 4;
-// Bounded waits: each try_wait may suspend the warp for up to WAIT_HINT_NS; after WAIT_TRIES
-// unsuccessful tries (about a second) the wait gives up and the kernel reports it.
-constexpr unsigned WAIT_HINT_NS = 20000;
-constexpr int WAIT_TRIES = 1 << 16;
-
 template <typename VT, typename IT> struct Stage {
     static constexpr int BPB = 128 * (int)(sizeof(VT) + sizeof(IT));  // bytes per block
     static constexpr int KB = STAGE_BYTES / BPB > 0 ? STAGE_BYTES / BPB : 1;
@@ -147,61 +143,6 @@ template <typename VT, typename IT> struct Stage {
     static constexpr int CTA_BYTES = SELL_WARPS * WARP_BYTES;
     static_assert(STAGES * 8 <= 128 && WARP_BYTES % 128 == 0, "stage layout");
 };
-
-__device__ __forceinline__ void mbar_init(unsigned a) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned a, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
-                 : "memory");
-}
-// global -> this CTA's shared memory; both addresses 16-byte aligned, bytes a multiple of 16
-__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes,
-                                         unsigned mbar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        ::"r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
-}
-__device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity) {
-    for (int i = 0; i < WAIT_TRIES; ++i) {
-        unsigned ok;
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; "
-            "selp.u32 %0, 1, 0, p; }"
-            : "=r"(ok) : "r"(a), "r"(parity), "r"(WAIT_HINT_NS) : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
-
-// Stream blocks from a shared-memory stage (same block layout as the global streams).
-template <typename VT> __device__ __forceinline__ VBlk<VT> vblk_smem(const VT *p, int blk, int lane);
-template <> __device__ __forceinline__ VBlk<double> vblk_smem<double>(const double *p, int blk,
-                                                                      int lane) {
-    const double2 *q = reinterpret_cast<const double2 *>(p);
-    VBlk<double> r;
-    r.a = q[(2 * blk) * 32 + lane];
-    r.b = q[(2 * blk + 1) * 32 + lane];
-    return r;
-}
-template <> __device__ __forceinline__ VBlk<float> vblk_smem<float>(const float *p, int blk,
-                                                                    int lane) {
-    VBlk<float> r;
-    r.a = reinterpret_cast<const float4 *>(p)[blk * 32 + lane];
-    return r;
-}
-template <typename IT> __device__ __forceinline__ CBlk<IT> cblk_smem(const IT *p, int blk, int lane);
-template <> __device__ __forceinline__ CBlk<int> cblk_smem<int>(const int *p, int blk, int lane) {
-    CBlk<int> r;
-    r.a = reinterpret_cast<const int4 *>(p)[blk * 32 + lane];
-    return r;
-}
-template <> __device__ __forceinline__ CBlk<short> cblk_smem<short>(const short *p, int blk,
-                                                                    int lane) {
-    CBlk<short> r;
-    r.a = reinterpret_cast<const uint2 *>(p)[blk * 32 + lane];
-    return r;
-}
 
 // SpMV.  Warps take slices in turn (grid-stride: the warps of the grid work on neighbouring
 // slices at any time, so the streams are read close to in order).  Each warp walks its slices
@@ -229,7 +170,7 @@ sell_spmv_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
     const unsigned sv0 = bar0 + 128, sc0 = bar0 + 128 + STAGES * ST::VBYTES;
     if (lane == 0) {
         for (int k = 0; k < STAGES; ++k) mbar_init(bar0 + 8 * k);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_init_fence();
     }
     __syncwarp();
     const uint64_t pl = policy_evict_last();
@@ -251,8 +192,7 @@ sell_spmv_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
         if (lane == 0) {
             const unsigned vb = (unsigned)(len * 128 * (int)sizeof(VT));
             const unsigned cb = (unsigned)(len * 128 * (int)sizeof(IT));
-            // the stage's last reads (generic proxy) come before the copy's writes
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            proxy_fence();  // the stage's last reads come before the copy's writes
             mbar_expect_tx(bar0 + 8 * k, vb + cb);
             bulk_g2s(sv0 + k * ST::VBYTES, vals + e0, vb, bar0 + 8 * k);
             bulk_g2s(sc0 + k * ST::CBYTES, cols + e0, cb, bar0 + 8 * k);
@@ -316,12 +256,13 @@ sell_spmv_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
             }
         };
         VT xs[2][4];
-        gather4(cblk_smem<IT>(pc, 0, lane), xs[0], 0);
+        gather4(CBlk<IT>::load_smem(pc, 0, lane), xs[0], 0);
 #pragma unroll
         for (int i = 0; i < KB; ++i) {
             if (i < len) {
-                if (i + 1 < len) gather4(cblk_smem<IT>(pc, i + 1, lane), xs[(i + 1) & 1], i + 1);
-                const VBlk<VT> vv = vblk_smem<VT>(pv, i, lane);
+                if (i + 1 < len)
+                    gather4(CBlk<IT>::load_smem(pc, i + 1, lane), xs[(i + 1) & 1], i + 1);
+                const VBlk<VT> vv = VBlk<VT>::load_smem(pv, i, lane);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) acc.add(vv.get(q), xs[i & 1][q]);
             }

@@ -32,6 +32,14 @@ template <> struct VBlk<double> {
         r.b = ld_stream(p + (2 * blk + 1) * 32 + lane, pol);
         return r;
     }
+    // the same block from a copy of the stream in shared memory
+    __device__ __forceinline__ static VBlk load_smem(const double *base, int blk, int lane) {
+        const double2 *p = reinterpret_cast<const double2 *>(base);
+        VBlk r;
+        r.a = p[(2 * blk) * 32 + lane];
+        r.b = p[(2 * blk + 1) * 32 + lane];
+        return r;
+    }
 };
 template <> struct VBlk<float> {
     float4 a;
@@ -41,6 +49,11 @@ template <> struct VBlk<float> {
     __device__ __forceinline__ static VBlk load(const float *base, int blk, int lane, uint64_t pol) {
         VBlk r;
         r.a = ld_stream(reinterpret_cast<const float4 *>(base) + blk * 32 + lane, pol);
+        return r;
+    }
+    __device__ __forceinline__ static VBlk load_smem(const float *base, int blk, int lane) {
+        VBlk r;
+        r.a = reinterpret_cast<const float4 *>(base)[blk * 32 + lane];
         return r;
     }
 };
@@ -75,6 +88,11 @@ template <> struct CBlk<int> {
         r.a = ld_stream(reinterpret_cast<const int4 *>(base) + blk * 32 + lane, pol);
         return r;
     }
+    __device__ __forceinline__ static CBlk load_smem(const int *base, int blk, int lane) {
+        CBlk r;
+        r.a = reinterpret_cast<const int4 *>(base)[blk * 32 + lane];
+        return r;
+    }
 };
 template <> struct CBlk<short> {
     // x of element q: xb = x + (the chunk's base column); the offset DELTA_NONE reads nothing
@@ -103,6 +121,11 @@ template <> struct CBlk<short> {
     __device__ __forceinline__ static CBlk load(const short *base, int blk, int lane, uint64_t pol) {
         CBlk r;
         r.a = ld_stream(reinterpret_cast<const uint2 *>(base) + blk * 32 + lane, pol);
+        return r;
+    }
+    __device__ __forceinline__ static CBlk load_smem(const short *base, int blk, int lane) {
+        CBlk r;
+        r.a = reinterpret_cast<const uint2 *>(base)[blk * 32 + lane];
         return r;
     }
 };
