@@ -87,7 +87,8 @@ typedef struct pava_opts {
     int precision;        /* pava_precision */
     int index_mode;       /* pava_index_mode */
     int lanes_per_row;    /* CSR: lanes per row group, 1, 2, 4, 8, 16 or 32 (default: from
-                             the mean row length, or from k for pava_spmm) */
+                             the mean row length, or from k for pava_spmm); SELL: lanes per
+                             row of pava_spmm, 4, 8 or 16 (default: from k) */
     int col_lanes;        /* CSR, pava_spmm: lanes of a group across the k right-hand sides,
                              a power of two <= lanes_per_row (default: from k) */
     int cols_per_lane;    /* CSR, pava_spmm: right-hand sides per lane, 1, 2 or 4; needs
@@ -168,9 +169,12 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
 pava_status pava_spmv(pava_handle *h, const void *x, void *y, void *stream);
 
 /* Y = A X for k right-hand sides: X is n x k and Y is m x k, both row-major with leading
- * dimensions ldx >= k and ldy >= k (elements), device memory.  CSR handles only (the
- * row-group kernel; FP64, or FP32C with float X and double Y), 1 <= k <= 128.  The reference
- * has no multi-vector product; k = 1 equals pava_spmv. */
+ * dimensions ldx >= k and ldy >= k (elements), device memory; FP64, or FP32C with float X and
+ * double Y.  CSR handles (the row-group kernel), 1 <= k <= 128, and SELL handles (a CTA per
+ * 32-row slice, the slice's streams in shared memory, opts.lanes_per_row = 4, 8 or 16 lanes
+ * per row across k; 0 = 4 for k <= 8, else 8), 1 <= k <= 64, k <= 8 with 4 lanes
+ * (PAVA_E_UNSUPPORTED_PARAMS past it).  The reference has no multi-vector product; k = 1
+ * equals pava_spmv. */
 pava_status pava_spmm(pava_handle *h, int k, const void *X, long long ldx, void *Y,
                       long long ldy, void *stream);
 /* pava_spmv split into its launches, for timing one kernel: stage 1 runs the format's SpMV

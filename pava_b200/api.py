@@ -94,7 +94,8 @@ class SpMatrix:
         return y
 
     def spmm(self, X, Y=None, stream=None):
-        """Y = A X for a row-major (n, k) CUDA tensor X (CSR handles); Y is (m, k) float64."""
+        """Y = A X for a row-major (n, k) CUDA tensor X (CSR handles, k <= 128; SELL handles,
+        k <= 64); Y is (m, k) float64."""
         torch = _torch()
         want = torch.float32 if self.precision == _abi.PREC_FP32C else torch.float64
         if X.dim() != 2 or X.dtype != want or not X.is_cuda or X.stride(1) != 1:

@@ -30,7 +30,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 GPU_SOURCES = ["api.cu", "k_support.cu", "k_cvr.cu", "k_csr5.cu", "k_group.cu", "noalloc.cu",
                "batch.cu", "k_gen.cu", "k_features.cu", "k_mlp.cu", "select.cu", "k_coo.cu",
-               "k_sell.cu"]
+               "k_sell.cu", "k_sell_spmm.cu"]
 HOST_SOURCES = ["host/gen.cpp", "host/mtx.cpp"]
 
 

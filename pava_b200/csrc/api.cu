@@ -519,7 +519,13 @@ pava_status pava_create(const pava_csr *A, int format, const pava_opts *opts, vo
         }
         h.L = 32LL * h.sigma * h.G;
     } else if (format == PAVA_FORMAT_SELL) {
-        // no shape options: a slice is 32 rows, its block 4 steps
+        // a slice is 32 rows, its block 4 steps; lanes_per_row: the SpMM's lanes per row
+        if (!(o.lanes_per_row == 0 || o.lanes_per_row == 4 || o.lanes_per_row == 8 ||
+              o.lanes_per_row == 16)) {
+            delete H;
+            return fail(PAVA_E_UNSUPPORTED_PARAMS, "SELL lanes_per_row must be 0, 4, 8 or 16");
+        }
+        h.lanes_per_row = o.lanes_per_row;
     } else {
         // 0 = derive per call (resolve_group_shape)
         h.lanes_per_row = o.lanes_per_row;
@@ -647,12 +653,20 @@ pava_status pava_spmm(pava_handle *H, int k, const void *X, long long ldx, void 
                       long long ldy, void *stream) {
     if (!H) return fail(PAVA_E_INVALID_ARG, "handle is NULL");
     pava::Handle &h = H->h;
-    if (h.format != PAVA_FORMAT_CSR)
-        return fail(PAVA_E_UNKNOWN_FORMAT, "pava_spmm needs a CSR handle");
+    if (h.format != PAVA_FORMAT_CSR && h.format != PAVA_FORMAT_SELL)
+        return fail(PAVA_E_UNKNOWN_FORMAT, "pava_spmm needs a CSR or SELL handle");
     if (k < 1 || k > 128) return fail(PAVA_E_INVALID_ARG, "k must be in [1, 128]");
     if (ldx < k || ldy < k) return fail(PAVA_E_INVALID_ARG, "ldx and ldy must be >= k");
     if (h.m == 0) return PAVA_SUCCESS;
     if (!X || !Y) return fail(PAVA_E_INVALID_ARG, "X or Y is NULL");
+    if (h.format == PAVA_FORMAT_SELL) {
+        if (pava::sell_spmm_lanes(h.lanes_per_row, k) == 0)
+            return fail(PAVA_E_UNSUPPORTED_PARAMS,
+                        "SELL SpMM takes k <= 64 (k <= 8 with 4 lanes per row)");
+        const cudaError_t e = pava::sell_spmm(h, X, ldx, Y, ldy, k, (cudaStream_t)stream);
+        if (e != cudaSuccess) return fail_cuda(e, "spmm launch");
+        return PAVA_SUCCESS;
+    }
     pava::Handle g;
     std::string why;
     if (!resolve_group_shape(h, k, g, why)) return fail(PAVA_E_UNSUPPORTED_PARAMS, why);

@@ -174,7 +174,8 @@ pava_status build_union(int count, const pava_csr *mats, cudaStream_t s, pava_ba
 }
 
 // Built-in candidate forms for k right-hand sides: for k = 1 the 32 forms of pava_variant in
-// their order (the selector's space); for k > 1 the row-group shapes (at most 72 for k <= 128).
+// their order (the selector's space); for k > 1 the row-group shapes (at most 72 for k <= 128)
+// and the SELL SpMM shapes (lanes per row x column form, at most 6).
 std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
     std::vector<std::pair<int, pava_opts>> c;
     auto base = [&]() {
@@ -219,6 +220,16 @@ std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
                     o.rows_per_tile = tr;  // a multiple of 8 * 32 / gl for every gl >= 2
                     c.push_back({PAVA_FORMAT_CSR, o});
                 }
+    }
+    // SELL: 4 (k <= 8), 8 or 16 lanes per row, 32-bit columns or 16-bit offsets where they reach
+    for (int g : {4, 8, 16}) {
+        if (pava::sell_spmm_lanes(g, k) == 0) continue;
+        for (int idx : {PAVA_INDEX_I32, PAVA_INDEX_AUTO}) {
+            pava_opts o = base();
+            o.lanes_per_row = g;
+            o.index_mode = idx;
+            c.push_back({PAVA_FORMAT_SELL, o});
+        }
     }
     return c;
 }
@@ -322,8 +333,12 @@ pava_status pava_batch_create_spmm(int count, const pava_csr *mats, int k, int f
     *out = nullptr;
     if (count < 1 || !mats) return bfail(PAVA_E_INVALID_ARG, "empty batch");
     if (k < 1 || k > 128) return bfail(PAVA_E_INVALID_ARG, "k must be in [1, 128]");
-    if (k > 1 && format >= 0 && format != PAVA_FORMAT_CSR)
-        return bfail(PAVA_E_UNKNOWN_FORMAT, "k > 1 right-hand sides need the CSR row-group form");
+    if (k > 1 && format >= 0 && format != PAVA_FORMAT_CSR && format != PAVA_FORMAT_SELL)
+        return bfail(PAVA_E_UNKNOWN_FORMAT,
+                     "k > 1 right-hand sides need the CSR row-group or the SELL form");
+    if (k > 1 && format == PAVA_FORMAT_SELL &&
+        pava::sell_spmm_lanes(opts ? opts->lanes_per_row : 0, k) == 0)
+        return bfail(PAVA_E_UNSUPPORTED_PARAMS, "SELL SpMM takes k <= 64 (k <= 8 with 4 lanes)");
     pava_batch *b = new (std::nothrow) pava_batch();
     if (!b) return bfail(PAVA_E_NOMEM, "host allocation failed");
     b->count = count;

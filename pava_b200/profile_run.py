@@ -112,6 +112,13 @@ def main():
             X = torch.from_numpy(M.uniform(A.n * a.k, seed=2, fp32=True)).reshape(A.n, a.k)
             X = X.to("cuda", x.dtype)
             Y = torch.empty((A.m, a.k), dtype=torch.float64, device="cuda")
+            try:  # a shape that cannot serve k is reported, not fatal
+                mat.spmm(X, Y)
+            except _abi.PavaError as e:
+                print(json.dumps({"matrix": a.matrix, "format": fmt, "opts": kw, "k": a.k,
+                                  "error": str(e)}))
+                mat.close()
+                continue
         s = torch.cuda.current_stream().cuda_stream
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(a.reps)]

@@ -300,23 +300,32 @@ def test_autotune_wave_balanced_csr5(cuda):
 def test_autotune_spmm(cuda, k):
     A = M.banded(50_000, 64, 24, seed=29)
     ents, best = autotune(A, k=k, reps=3)
-    assert all(e["format"] == "csr" for e in ents)
-    assert all(e["opts"]["col_lanes"] * e["opts"]["cols_per_lane"] >= k for e in ents)
-    assert ents[best]["ms"] > 0
+    assert {e["format"] for e in ents} == {"csr", "sell"}
+    assert all(e["opts"]["col_lanes"] * e["opts"]["cols_per_lane"] >= k
+               for e in ents if e["format"] == "csr")
+    # SELL: 4 lanes per row only for k <= 8, 8 and 16 always; each with 32-bit / 16-bit columns
+    sell = {(e["opts"]["lanes_per_row"], e["opts"]["index_mode"]) for e in ents
+            if e["format"] == "sell"}
+    assert sell == {(g, m) for g in ((4, 8, 16) if k <= 8 else (8, 16))
+                    for m in (_abi.INDEX_I32, _abi.INDEX_AUTO)}
+    assert all(e["ms"] > 0 and e["status"] == 0 for e in ents)
+    assert ents[best]["ms"] == min(e["ms"] for e in ents)
 
 
 # ---- the batching configuration at full size ----------------------------------------------
 
 def test_config4_banded_full(cuda):
-    """1,048,576-row banded matrix (half-bandwidth 64, 24 per row), k = 1, 8, 32."""
+    """1,048,576-row banded matrix (half-bandwidth 64, 24 per row), k = 1, 8, 32, row groups
+    and SELL."""
     torch = cuda
     A = M.banded(1_048_576, 64, 24, seed=3)
     for k in (1, 8, 32):
         X, Xd = _x(torch, A.n, k, seed=30 + k)
-        Y = SpMatrix(A, "csr").spmm(Xd).cpu().numpy()
-        for j in sorted({0, k // 2, k - 1}):
-            yr, ab = O.csr_ref(A.rp, A.ci, A.v, np.ascontiguousarray(X[:, j]))
-            assert O.rel_error(np.ascontiguousarray(Y[:, j]), yr, ab, TOL)[0] == 0
+        for fmt in ("csr", "sell"):
+            Y = SpMatrix(A, fmt).spmm(Xd).cpu().numpy()
+            for j in sorted({0, k // 2, k - 1}):
+                yr, ab = O.csr_ref(A.rp, A.ci, A.v, np.ascontiguousarray(X[:, j]))
+                assert O.rel_error(np.ascontiguousarray(Y[:, j]), yr, ab, TOL)[0] == 0
 
 
 # ---- batches with k right-hand sides ------------------------------------------------------
@@ -344,15 +353,18 @@ def _check_batch_cols(mats, b, X, Y, tol, cols=None):
 
 
 @pytest.mark.parametrize("k", [2, 8, 13, 32])
-@pytest.mark.parametrize("fmt", ["csr", "auto"])
+@pytest.mark.parametrize("fmt", ["csr", "sell", "auto"])
 def test_batch_spmm_every_matrix_and_column(cuda, k, fmt):
     """k right-hand sides per matrix over the uneven batch (with an all-empty, a rectangular
     and a 1 x 1 matrix), one persistent launch, then the same launch captured and replayed."""
     torch = cuda
     mats = _batch_mats(60, seed=51)
+    if fmt == "sell":  # the union's Poisson rows pad 1.85x: SELL takes it
+        from pava_b200.batch_bench import union_csr
+        assert M.sell_accepts(union_csr(mats))
     b = Batch(mats, fmt, k=k)
     if fmt == "auto":
-        assert b.chosen()[0] == "csr" or k == 1
+        assert b.chosen()[0] in ("csr", "sell")
     X = _batch_X(torch, b, k, seed=52)
     Y = b.spmm(X)
     _check_batch_cols(mats, b, X, Y, TOL)

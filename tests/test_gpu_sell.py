@@ -131,3 +131,80 @@ def test_sell_empty_rows_ignore_nonfinite_x(cuda):
     y, _ = _run(cuda, A, x)
     assert np.all(np.isfinite(y)) and np.all(y[np.diff(A.rp) == 0] == 0.0)
     _check(y, A, np.where(read, x, 0.0), 1e-12)
+
+
+def _spmm_check(torch, A, k, tol, ldx_pad=0, **kw):
+    """Y = A X on a SELL handle against the oracle, column by column; X row-major n x k with
+    leading dimension k + ldx_pad."""
+    fp32 = kw.get("precision") == _abi.PREC_FP32C
+    Xh = M.uniform(A.n * (k + ldx_pad), seed=40 + k, fp32=fp32).reshape(A.n, k + ldx_pad)
+    Xd = torch.from_numpy(Xh).to("cuda", torch.float32 if fp32 else torch.float64)[:, :k]
+    mat = SpMatrix(A, "sell", **kw)
+    Y = torch.full((A.m, k), float("nan"), dtype=torch.float64, device="cuda")
+    mat.spmm(Xd, Y)
+    Yh = Y.cpu().numpy()
+    mat.close()
+    for j in range(k):
+        xj = np.ascontiguousarray(Xh[:, j])
+        yr, ab = O.csr_ref(A.rp, A.ci, A.v, xj)
+        bad, mx, _ = O.rel_error(np.ascontiguousarray(Yh[:, j]), yr, ab, tol)
+        assert bad == 0, f"column {j}: {bad} rows above {tol}, max rel {mx}"
+
+
+@pytest.mark.parametrize("k", [1, 3, 8, 16, 32, 33, 64])
+@pytest.mark.parametrize("index_mode", [_abi.INDEX_I32, _abi.INDEX_AUTO], ids=["i32", "auto"])
+def test_sell_spmm_fp64(cuda, k, index_mode):
+    """Every k path: 1 column per lane (k <= 8), pairs of columns per read (even k up to 64),
+    single columns (odd k); a banded matrix with some empty slices."""
+    A = M.banded(20_000, 64, 24, seed=41)
+    keep = np.ones(A.m, bool)
+    keep[3_200:3_300] = False  # empty rows: three whole empty slices
+    lens = np.where(keep, np.diff(A.rp), 0)
+    sel = np.repeat(keep, np.diff(A.rp))
+    B = M.from_arrays(A.m, A.n, np.concatenate([[0], np.cumsum(lens)]).astype(np.int32),
+                      A.ci[sel], A.v[sel])
+    assert M.sell_accepts(B)
+    _spmm_check(cuda, B, k, 1e-12, index_mode=index_mode)
+
+
+@pytest.mark.parametrize("k", [8, 32])
+def test_sell_spmm_fp32c_and_strided_x(cuda, k):
+    A = M.stencil27(20, seed=42)
+    A.v = A.v.astype(np.float32).astype(np.float64)
+    _spmm_check(cuda, A, k, 1e-9, precision=_abi.PREC_FP32C, index_mode=_abi.INDEX_AUTO)
+    _spmm_check(cuda, A, k, 1e-12, ldx_pad=5)  # X with a leading dimension of k + 5
+
+
+def test_sell_spmm_shapes(cuda):
+    """Slices longer than a piece, ragged slices and empty-slice runs, k = 32."""
+    for name in ("long_equal_rows", "empty_slice_runs", "thirty_three", "ragged_blocks"):
+        _spmm_check(cuda, CASES[name](), 32, 1e-12)
+
+
+def test_sell_spmm_k_limit(cuda):
+    A = M.banded(2_000, 8, 5, seed=43)
+    mat = SpMatrix(A, "sell")
+    X = cuda.zeros((A.n, 65), dtype=cuda.float64, device="cuda")
+    with pytest.raises(_abi.PavaError) as e:
+        mat.spmm(X)
+    assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
+
+
+@pytest.mark.parametrize("lanes,k", [(4, 1), (4, 5), (4, 8), (8, 8), (16, 16), (16, 31),
+                                     (16, 64)])
+def test_sell_spmm_lanes_per_row(cuda, lanes, k):
+    """Every lanes-per-row shape the SpMM offers, even and odd k."""
+    A = M.banded(10_000, 32, 12, seed=44)
+    _spmm_check(cuda, A, k, 1e-12, lanes_per_row=lanes)
+
+
+def test_sell_spmm_lanes_refused(cuda):
+    A = M.banded(2_000, 8, 5, seed=45)
+    with pytest.raises(_abi.PavaError) as e:
+        SpMatrix(A, "sell", lanes_per_row=2)
+    assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
+    mat = SpMatrix(A, "sell", lanes_per_row=4)
+    X = cuda.zeros((A.n, 9), dtype=cuda.float64, device="cuda")
+    with pytest.raises(_abi.PavaError) as e:
+        mat.spmm(X)  # 4 lanes per row take k <= 8
+    assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
