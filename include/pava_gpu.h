@@ -172,7 +172,7 @@ pava_status pava_spmv(pava_handle *h, const void *x, void *y, void *stream);
  * dimensions ldx >= k and ldy >= k (elements), device memory; FP64, or FP32C with float X and
  * double Y.  CSR handles (the row-group kernel), 1 <= k <= 128, and SELL handles (a CTA per
  * 32-row slice, the slice's streams in shared memory, opts.lanes_per_row = 4, 8 or 16 lanes
- * per row across k; 0 = 4 for k <= 8, else 8), 1 <= k <= 64, k <= 8 with 4 lanes
+ * per row across k; 0 = 4 for k <= 16, else 8), 1 <= k <= 64, k <= 32 with 4 lanes
  * (PAVA_E_UNSUPPORTED_PARAMS past it).  The reference has no multi-vector product; k = 1
  * equals pava_spmv. */
 pava_status pava_spmm(pava_handle *h, int k, const void *X, long long ldx, void *Y,

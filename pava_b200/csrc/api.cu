@@ -662,7 +662,7 @@ pava_status pava_spmm(pava_handle *H, int k, const void *X, long long ldx, void 
     if (h.format == PAVA_FORMAT_SELL) {
         if (pava::sell_spmm_lanes(h.lanes_per_row, k) == 0)
             return fail(PAVA_E_UNSUPPORTED_PARAMS,
-                        "SELL SpMM takes k <= 64 (k <= 8 with 4 lanes per row)");
+                        "SELL SpMM takes k <= 64 (k <= 32 with 4 lanes per row)");
         const cudaError_t e = pava::sell_spmm(h, X, ldx, Y, ldy, k, (cudaStream_t)stream);
         if (e != cudaSuccess) return fail_cuda(e, "spmm launch");
         return PAVA_SUCCESS;

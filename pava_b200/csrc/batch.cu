@@ -175,7 +175,7 @@ pava_status build_union(int count, const pava_csr *mats, cudaStream_t s, pava_ba
 
 // Built-in candidate forms for k right-hand sides: for k = 1 the 32 forms of pava_variant in
 // their order (the selector's space); for k > 1 the row-group shapes (at most 72 for k <= 128)
-// and the SELL SpMM shapes (lanes per row x column form, at most 6).
+// and the SELL SpMM shapes (lanes per row x column form, at most 4).
 std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
     std::vector<std::pair<int, pava_opts>> c;
     auto base = [&]() {
@@ -221,8 +221,10 @@ std::vector<std::pair<int, pava_opts>> candidates(int k, int precision) {
                     c.push_back({PAVA_FORMAT_CSR, o});
                 }
     }
-    // SELL: 4 (k <= 8), 8 or 16 lanes per row, 32-bit columns or 16-bit offsets where they reach
-    for (int g : {4, 8, 16}) {
+    // SELL: 4 (k <= 32) or 8 lanes per row, 32-bit columns or 16-bit offsets where they reach
+    // (16 lanes per row, an option of pava_create, was never faster on the banded, stencil and
+    // batch matrices)
+    for (int g : {4, 8}) {
         if (pava::sell_spmm_lanes(g, k) == 0) continue;
         for (int idx : {PAVA_INDEX_I32, PAVA_INDEX_AUTO}) {
             pava_opts o = base();
@@ -338,7 +340,7 @@ pava_status pava_batch_create_spmm(int count, const pava_csr *mats, int k, int f
                      "k > 1 right-hand sides need the CSR row-group or the SELL form");
     if (k > 1 && format == PAVA_FORMAT_SELL &&
         pava::sell_spmm_lanes(opts ? opts->lanes_per_row : 0, k) == 0)
-        return bfail(PAVA_E_UNSUPPORTED_PARAMS, "SELL SpMM takes k <= 64 (k <= 8 with 4 lanes)");
+        return bfail(PAVA_E_UNSUPPORTED_PARAMS, "SELL SpMM takes k <= 64 (k <= 32 with 4 lanes)");
     pava_batch *b = new (std::nothrow) pava_batch();
     if (!b) return bfail(PAVA_E_NOMEM, "host allocation failed");
     b->count = count;

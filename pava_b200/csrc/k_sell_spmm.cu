@@ -32,9 +32,13 @@ namespace {
 
 // The shape of G lanes per row: 32 G threads per CTA (32 rows), 32 / G CTAs per SM (32 warps),
 // pieces of 2 G blocks (about 200 KB of stages per SM for FP64 values and 32-bit columns).
+#ifndef PAVA_SELL_SPMM_KB2
+#define PAVA_SELL_SPMM_KB2 2
+#endif
 template <int G> struct SpmmShape {
     static_assert(G == 4 || G == 8 || G == 16, "lanes per row");
-    static constexpr int THREADS = 32 * G, CTAS_PER_SM = 32 / G, KB = 2 * G;
+    static constexpr int THREADS = 32 * G, CTAS_PER_SM = 32 / G;
+    static constexpr int KB = PAVA_SELL_SPMM_KB2 * G / 2 > 0 ? PAVA_SELL_SPMM_KB2 * G / 2 : 1;
 };
 template <typename VT, typename IT, int G> struct SpmmStage {
     static constexpr int VBYTES = SpmmShape<G>::KB * 128 * (int)sizeof(VT);
@@ -100,14 +104,23 @@ sell_spmm_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
     bool colok[KPL];
 #pragma unroll
     for (int p = 0; p < KPL; ++p) colok[p] = spmm_col<G, VW>(lg, p) < k;
-    const long long step = gridDim.x;
+#ifndef PAVA_SELL_SPMM_CONTIG
+#define PAVA_SELL_SPMM_CONTIG 0
+#endif
+    // the CTA's slices: in turn over the grid, or a contiguous run (neighbouring slices share
+    // most of their X rows, which then stay in L1)
+    const long long step = PAVA_SELL_SPMM_CONTIG ? 1 : gridDim.x;
+    const long long s_first =
+        PAVA_SELL_SPMM_CONTIG ? nslices * blockIdx.x / gridDim.x : (long long)blockIdx.x;
+    const long long s_end =
+        PAVA_SELL_SPMM_CONTIG ? nslices * (blockIdx.x + 1) / gridDim.x : nslices;
 
     // producer cursor (the CTA's slices with blocks; thread 0 issues the copies)
-    long long ps = blockIdx.x;
+    long long ps = s_first;
     int pb = 0;
     SellSlice pm{0, 0, 0, 0u};
     auto p_find = [&]() {
-        for (; ps < nslices; ps += step) {
+        for (; ps < s_end; ps += step) {
             pm = meta[ps];
             if (pm.nblk > 0) break;
         }
@@ -134,13 +147,13 @@ sell_spmm_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
     int pending = 0;
 #pragma unroll
     for (int kk = 0; kk < 2; ++kk)
-        if (ps < nslices) {
+        if (ps < s_end) {
             issue(kk);
             ++pending;
         }
 
     // consumer cursor; the rows of empty slices are written as zeros
-    long long cs = blockIdx.x;
+    long long cs = s_first;
     int cb = 0;
     SellSlice cm{0, 0, 0, 0u};
     auto store_row = [&](long long slice, const double (&acc)[KPL]) {
@@ -161,7 +174,7 @@ sell_spmm_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
         double zero[KPL];
 #pragma unroll
         for (int p = 0; p < KPL; ++p) zero[p] = 0.0;
-        for (; cs < nslices; cs += step) {
+        for (; cs < s_end; cs += step) {
             cm = meta[cs];
             if (cm.nblk > 0) break;
             store_row(cs, zero);
@@ -173,7 +186,7 @@ sell_spmm_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
     double acc[KPL];
 #pragma unroll
     for (int p = 0; p < KPL; ++p) acc[p] = 0.0;
-    while (cs < nslices) {
+    while (cs < s_end) {
         // every thread waits (bounded); the CTA gives up together if any thread did
         const bool ok = mbar_wait(bar0 + 8 * kk, (phases >> kk) & 1u);
         if (__syncthreads_or(!ok)) {
@@ -226,7 +239,7 @@ sell_spmm_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
             c_find();
         }
         __syncthreads();  // every thread is done with stage kk
-        if (ps < nslices) {
+        if (ps < s_end) {
             issue(kk);
             ++pending;
         }
@@ -282,6 +295,8 @@ cudaError_t spmm_k(const Handle &h, const VT *X, long long ldx, double *Y, long 
     if (g == 4) {
         if (k <= 4) return spmm_vw<VT, IT, 4, 1>(h, X, ldx, Y, ldy, k, s);
         if (k <= 8) return spmm_vw<VT, IT, 4, 2>(h, X, ldx, Y, ldy, k, s);
+        if (k <= 16) return spmm_vw<VT, IT, 4, 4>(h, X, ldx, Y, ldy, k, s);
+        if (k <= 32) return spmm_vw<VT, IT, 4, 8>(h, X, ldx, Y, ldy, k, s);
     } else if (g == 8) {
         if (k <= 8) return spmm_vw<VT, IT, 8, 1>(h, X, ldx, Y, ldy, k, s);
         if (k <= 16) return spmm_vw<VT, IT, 8, 2>(h, X, ldx, Y, ldy, k, s);

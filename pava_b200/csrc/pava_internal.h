@@ -134,13 +134,13 @@ cudaError_t sell_fill(Handle &h, const int *rp, const int *ci, const double *v,
                       const int *d_blk_off, int *ovf, cudaStream_t s);
 cudaError_t sell_spmv(const Handle &h, const void *x, void *y, cudaStream_t s);
 // SELL SpMM, Y = A X with X row-major n x k; leading dimensions ldx, ldy in elements.  Lanes per
-// row (h.lanes_per_row): 4 (k <= 8), 8 (k <= 64) or 16 (k <= 64); 0 = 4 for k <= 8, else 8.
+// row (h.lanes_per_row): 4 (k <= 32), 8 (k <= 64) or 16 (k <= 64); 0 = 4 for k <= 16, else 8.
 // sell_spmm_lanes gives the lanes it uses for k, 0 when the handle's choice cannot serve k
 // (sell_spmm then returns cudaErrorInvalidValue).
 constexpr int SELL_SPMM_MAX_K = 64;
 inline int sell_spmm_lanes(int lanes_per_row, int k) {
-    const int g = lanes_per_row ? lanes_per_row : (k <= 8 ? 4 : 8);
-    if (g == 4) return k <= 8 ? 4 : 0;
+    const int g = lanes_per_row ? lanes_per_row : (k <= 16 ? 4 : 8);
+    if (g == 4) return k <= 32 ? 4 : 0;
     if (g == 8 || g == 16) return k <= SELL_SPMM_MAX_K ? g : 0;
     return 0;
 }

@@ -303,11 +303,10 @@ def test_autotune_spmm(cuda, k):
     assert {e["format"] for e in ents} == {"csr", "sell"}
     assert all(e["opts"]["col_lanes"] * e["opts"]["cols_per_lane"] >= k
                for e in ents if e["format"] == "csr")
-    # SELL: 4 lanes per row only for k <= 8, 8 and 16 always; each with 32-bit / 16-bit columns
+    # SELL: 4 (k <= 32) and 8 lanes per row, each with 32-bit / 16-bit columns
     sell = {(e["opts"]["lanes_per_row"], e["opts"]["index_mode"]) for e in ents
             if e["format"] == "sell"}
-    assert sell == {(g, m) for g in ((4, 8, 16) if k <= 8 else (8, 16))
-                    for m in (_abi.INDEX_I32, _abi.INDEX_AUTO)}
+    assert sell == {(g, m) for g in (4, 8) for m in (_abi.INDEX_I32, _abi.INDEX_AUTO)}
     assert all(e["ms"] > 0 and e["status"] == 0 for e in ents)
     assert ents[best]["ms"] == min(e["ms"] for e in ents)
 

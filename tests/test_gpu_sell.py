@@ -190,8 +190,8 @@ def test_sell_spmm_k_limit(cuda):
     assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
 
 
-@pytest.mark.parametrize("lanes,k", [(4, 1), (4, 5), (4, 8), (8, 8), (16, 16), (16, 31),
-                                     (16, 64)])
+@pytest.mark.parametrize("lanes,k", [(4, 1), (4, 5), (4, 8), (4, 16), (4, 27), (4, 32), (8, 8),
+                                     (16, 16), (16, 31), (16, 64)])
 def test_sell_spmm_lanes_per_row(cuda, lanes, k):
     """Every lanes-per-row shape the SpMM offers, even and odd k."""
     A = M.banded(10_000, 32, 12, seed=44)
@@ -204,7 +204,7 @@ def test_sell_spmm_lanes_refused(cuda):
         SpMatrix(A, "sell", lanes_per_row=2)
     assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
     mat = SpMatrix(A, "sell", lanes_per_row=4)
-    X = cuda.zeros((A.n, 9), dtype=cuda.float64, device="cuda")
+    X = cuda.zeros((A.n, 33), dtype=cuda.float64, device="cuda")
     with pytest.raises(_abi.PavaError) as e:
-        mat.spmm(X)  # 4 lanes per row take k <= 8
+        mat.spmm(X)  # 4 lanes per row take k <= 32
     assert e.value.status == _abi.E_UNSUPPORTED_PARAMS
