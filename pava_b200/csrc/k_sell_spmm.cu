@@ -8,7 +8,7 @@
 // per nonzero, and each thread keeps its KPL sums in registers for the whole slice.
 //
 // The slice's value and column streams come into shared memory by bulk asynchronous copies
-// (k_bulk.cuh), 2 G blocks per piece, two pieces in flight per CTA: thread 0 issues the
+// (k_bulk.cuh), G blocks per piece, two pieces in flight per CTA: thread 0 issues the
 // copies of the piece after next while the CTA sums the current one.  A row's four elements of
 // a block are one 16-byte shared-memory read per stream (the 8 lanes of the row read the same
 // address: a broadcast), where the row-group kernel (k_group.cu) passes every element to the
@@ -31,14 +31,13 @@ namespace pava {
 namespace {
 
 // The shape of G lanes per row: 32 G threads per CTA (32 rows), 32 / G CTAs per SM (32 warps),
-// pieces of 2 G blocks (about 200 KB of stages per SM for FP64 values and 32-bit columns).
-#ifndef PAVA_SELL_SPMM_KB2
-#define PAVA_SELL_SPMM_KB2 2
-#endif
+// pieces of G blocks (about 100 KB of stages per SM for FP64 values and 32-bit columns, which
+// leaves L1 room for the X rows neighbouring slices share; pieces of 2 G blocks were 5-10 %
+// slower, of G / 2 blocks 4-7 % slower).
+constexpr int SPMM_UNROLL = 2;  // blocks of a piece unrolled together
 template <int G> struct SpmmShape {
     static_assert(G == 4 || G == 8 || G == 16, "lanes per row");
-    static constexpr int THREADS = 32 * G, CTAS_PER_SM = 32 / G;
-    static constexpr int KB = PAVA_SELL_SPMM_KB2 * G / 2 > 0 ? PAVA_SELL_SPMM_KB2 * G / 2 : 1;
+    static constexpr int THREADS = 32 * G, CTAS_PER_SM = 32 / G, KB = G;
 };
 template <typename VT, typename IT, int G> struct SpmmStage {
     static constexpr int VBYTES = SpmmShape<G>::KB * 128 * (int)sizeof(VT);
@@ -104,16 +103,9 @@ sell_spmm_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
     bool colok[KPL];
 #pragma unroll
     for (int p = 0; p < KPL; ++p) colok[p] = spmm_col<G, VW>(lg, p) < k;
-#ifndef PAVA_SELL_SPMM_CONTIG
-#define PAVA_SELL_SPMM_CONTIG 0
-#endif
-    // the CTA's slices: in turn over the grid, or a contiguous run (neighbouring slices share
-    // most of their X rows, which then stay in L1)
-    const long long step = PAVA_SELL_SPMM_CONTIG ? 1 : gridDim.x;
-    const long long s_first =
-        PAVA_SELL_SPMM_CONTIG ? nslices * blockIdx.x / gridDim.x : (long long)blockIdx.x;
-    const long long s_end =
-        PAVA_SELL_SPMM_CONTIG ? nslices * (blockIdx.x + 1) / gridDim.x : nslices;
+    // the CTA's slices, in turn over the grid (a contiguous run of slices per CTA, whose
+    // neighbours share X rows, was measured slower on the stencil)
+    const long long step = gridDim.x, s_first = blockIdx.x, s_end = nslices;
 
     // producer cursor (the CTA's slices with blocks; thread 0 issues the copies)
     long long ps = s_first;
@@ -202,7 +194,7 @@ sell_spmm_kernel(const SellSlice *__restrict__ meta, const VT *__restrict__ vals
         const VT *pv = sv + kk * (ST::VBYTES / (int)sizeof(VT));
         const IT *pc = sc + kk * (ST::CBYTES / (int)sizeof(IT));
         const int xbase = sizeof(IT) == 2 ? cm.colbase : 0;  // base of the 16-bit offsets
-#pragma unroll 2
+#pragma unroll SPMM_UNROLL
         for (int i = 0; i < len; ++i) {
             int c[4];
             row_cols(pc, i, r, c);
