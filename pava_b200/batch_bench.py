@@ -10,8 +10,8 @@ graph, and a banded matrix with k right-hand sides; forms picked by the autotune
   union is autotuned (pava_autotune over its candidates, k = 1), converted into the winner,
   captured into a CUDA graph and replayed.
 * banded: 1,048,576 rows, half-bandwidth 64, 24 distinct columns per row, X row-major n x k
-  for k in {1, 8, 32}; the CSR row-group shape (lanes per row, lanes across k, columns per
-  lane, rows per tile) is autotuned per k.
+  for k in {1, 8, 32}; the form is autotuned per k (k > 1: the CSR row-group shapes -- lanes
+  per row, lanes across k, columns per lane, rows per tile -- and the SELL SpMM shapes).
 * batch_spmm: the 4,096-matrix batch with k in {8, 32} right-hand sides per matrix, autotuned
   for k, one persistent launch captured into a CUDA graph and replayed.
 
@@ -161,9 +161,9 @@ def run_banded(torch, rows, ks, reps, peak):
         X = M.uniform(A.n * k, seed=60 + k).reshape(A.n, k)
         Xd = torch.from_numpy(X).cuda()
         Y = torch.empty((A.m, k), dtype=torch.float64, device="cuda")
-        if e["format"] == "csr":
+        if k > 1:  # a CSR row-group or a SELL SpMM shape
             ms, _ = time_it(torch, lambda: mat.spmm(Xd, Y), reps)
-        else:  # k = 1 on a CVR / CSR5 form
+        else:
             ms, _ = time_it(torch, lambda: mat.spmv(Xd.reshape(-1), Y.reshape(-1)), reps)
         y0 = SpMatrix(A, "csr", lanes_per_row=8).spmv(Xd[:, 0].contiguous()).cpu().numpy()
         mx = float(np.max(np.abs(Y[:, 0].cpu().numpy() - y0)))
