@@ -518,7 +518,9 @@ def small_form(torch, stream, peak, reps=15):
     latency-bound) and the banded matrix (1,048,576 rows, half-bandwidth 64, 24 per row).
     Forms: CSR5 sigma 16, CVR steps 32, SELL with 32-bit columns and with 16-bit offsets; the
     fastest is reported with its GB/s (compulsory bytes, 12 per nonzero) and fraction of the
-    copy bandwidth."""
+    copy bandwidth.  Then SpMM on the banded matrix with k = 8 and 32 right-hand sides (X and Y
+    row-major, compulsory bytes 12 per nonzero + 8k per row of X and Y): the best row-group
+    shape of the autotuner's earlier runs against the SELL SpMM."""
     from pava_b200 import _abi
     from pava_b200 import matrices as M
     from pava_b200.api import SpMatrix
@@ -552,7 +554,40 @@ def small_form(torch, stream, peak, reps=15):
             out[key] = {"rows": A.m, "nnz": A.nnz, "form": best, "ms": round(forms[best], 5),
                         "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4),
                         "forms_ms": {k: round(v, 5) for k, v in forms.items()}}
-        out["l2"] = "flushed before every SpMV (256 MB write)"
+        # SpMM on the banded matrix: k = 8 and 32 right-hand sides, X and Y row-major, the best
+        # row-group shape against the SELL SpMM
+        A = M.banded(1_048_576, 64, 24)
+        for k, shapes in ((8, (("csr", dict(lanes_per_row=4, col_lanes=4, cols_per_lane=2,
+                                             rows_per_tile=32)),
+                               ("sell", dict(lanes_per_row=4)))),
+                          (32, (("csr", dict(lanes_per_row=8, col_lanes=8, cols_per_lane=4,
+                                              rows_per_tile=16)),
+                                ("sell", dict(lanes_per_row=8))))):
+            X = torch.from_numpy(M.uniform(A.n * k, seed=6)).cuda().reshape(A.n, k)
+            Y = torch.empty((A.m, k), dtype=torch.float64, device="cuda")
+            alg = A.nnz * 12.0 + 4.0 * (A.m + 1) + 8.0 * k * (A.n + A.m)
+            forms = {}
+            for fmt, kw in shapes:
+                mat = SpMatrix(A, fmt, **kw)
+                ts = []
+                with torch.cuda.stream(stream):
+                    for r in range(reps + 3):
+                        flush.fill_(float(r))
+                        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        a.record(stream)
+                        mat.spmm(X, Y, stream=stream)
+                        b.record(stream)
+                        b.synchronize()
+                        if r >= 3:
+                            ts.append(a.elapsed_time(b))
+                mat.close()
+                forms[fmt] = float(np.median(ts))
+            best = min(forms, key=forms.get)
+            gbs = alg / (forms[best] * 1e-3) / 1e9
+            out[f"banded_spmm_k{k}"] = {"form": best, "ms": round(forms[best], 5),
+                                        "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4),
+                                        "forms_ms": {f: round(v, 5) for f, v in forms.items()}}
+        out["l2"] = "flushed before every SpMV / SpMM (256 MB write)"
         return out
     except Exception as e:  # a side measurement; the headline line stands without it
         return {"unavailable": f"failed: {e}"}
