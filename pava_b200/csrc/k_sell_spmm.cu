@@ -10,10 +10,10 @@
 // The slice's value and column streams come into shared memory by bulk asynchronous copies
 // (k_bulk.cuh), G blocks per piece, two pieces in flight per CTA: thread 0 issues the
 // copies of the piece after next while the CTA sums the current one.  A row's four elements of
-// a block are one 16-byte shared-memory read per stream (the 8 lanes of the row read the same
+// a block are one 16-byte shared-memory read per stream (the G lanes of the row read the same
 // address: a broadcast), where the row-group kernel (k_group.cu) passes every element to the
-// lanes of its row by shuffles.  Padding elements (value 0, no column) load X row 0 or the
-// slice's base row and add nothing.
+// lanes of its row by shuffles.  Padding elements (value 0, no column) read X row 0 and add
+// nothing.
 //
 // No counterpart in the reference (its SpMV takes one vector; main.cpp:554-587 runs one matrix
 // and one vector at a time).
