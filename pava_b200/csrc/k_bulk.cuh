@@ -3,8 +3,9 @@
 //
 // A copy is issued by one thread: mbar_expect_tx(bar, bytes) arrives on the barrier and adds
 // the bytes it waits for, then bulk_g2s copies (global -> this CTA's own shared memory only,
-// untiled, no cache-hint operand; both addresses 16-byte aligned, the size a multiple of 16).  The phase completes when all the bytes have landed; consumers wait on its parity.
-// Every wait is bounded: mbarrier.try_wait with a suspend hint, at most WAIT_TRIES tries
+// untiled, no cache-hint operand; both addresses 16-byte aligned, the size a multiple of 16).
+// The phase completes when all the bytes have landed; consumers wait on its parity.  Every
+// wait is bounded: mbarrier.try_wait with a suspend hint, at most BULK_WAIT_TRIES tries
 // (about a second), and the caller decides what to do when it gives up.
 #pragma once
 #include <cstdint>
