@@ -57,7 +57,8 @@ def parse():
                    help="skip the FP64 vs FP32C comparison on the 27-point stencil")
     p.add_argument("--no-small", action="store_true",
                    help="skip the 512^2 Laplacian / banded measurement")
-    p.add_argument("--variants", default="cvr:steps=64,cvr:steps=128,csr5:sigma=16,csr5:sigma=32",
+    p.add_argument("--variants",
+                   default="cvr:steps=64,cvr:steps=128,csr5:sigma=16,csr5:sigma=32,sell:",
                    help="FP64 candidates for the chosen variant")
     return p.parse_args()
 
@@ -298,9 +299,14 @@ def main():
     # candidates: FP64 CVR / CSR5 forms (the chosen one) and the plain FP64 CSR kernel
     variants = {}
     mats = {}
+    refused = {}
     for fmt, kw in parse_variants(args.variants):
         name = fmt + "".join(f"_{k}{v}" for k, v in kw.items())
-        mats[name] = SpMatrix(A, fmt, **kw)
+        try:
+            mats[name] = SpMatrix(A, fmt, **kw)
+        except _abi.PavaError as e:  # a form that does not take the matrix (SELL: padding)
+            refused[name] = str(e)
+            continue
         variants[name] = {"ms": time_variant(mats[name], 10),
                           "convert_ms": mats[name].info()["convert_ms"]}
     plain = SpMatrix(A, "csr")
@@ -429,6 +435,7 @@ def main():
                            "GB/s": round(alg / (plain_ms * 1e-3) / 1e9, 3)},
             "variants": {k: {"ms": round(v["ms"], 6), "GB/s": round(alg / (v["ms"] * 1e-3) / 1e9, 3),
                              "convert_ms": round(v["convert_ms"], 3)} for k, v in variants.items()},
+            "variants_refused": refused,
             "max_rel_diff_vs_plain_csr": max_rel_vs_plain,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 3), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s",
