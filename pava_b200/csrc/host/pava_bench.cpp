@@ -1,9 +1,12 @@
 // pava_bench: the benchmark loop of pava's main.cpp (conduct_benchmark, main.cpp:554-587) for
 // the CVR and CSR5 sections, with the GPU engine in place of the AVX-512 one.
 //
-//   pava_bench <matrix.mtx> [iterations]
-//   pava_bench --laplace <grid> [iterations]
-//   pava_bench --powerlaw <rows> [iterations]
+//   pava_bench <matrix.mtx> [iterations] [--sell]
+//   pava_bench --laplace <grid> [iterations] [--sell]
+//   pava_bench --powerlaw <rows> [iterations] [--sell]
+//
+// --sell adds a third section for the SELL form (no counterpart in main.cpp), or one line
+// saying why the form refuses the matrix.
 //
 // Per section: y is zeroed (initVectors, basicMatrix.cpp:499-520), the engine entry point
 // converts, runs the checked SpMV into y and times `iterations` more (printing the
@@ -167,9 +170,14 @@ bool generate(const char *kind, int size, Csr &A) {
 }  // namespace
 
 int main(int argc, char **argv) {
+    bool with_sell = false;  // a trailing --sell asks for the SELL section
+    if (argc >= 2 && !strcmp(argv[argc - 1], "--sell")) {
+        with_sell = true;
+        --argc;
+    }
     if (argc < 2) {
         fprintf(stderr, "usage: %s <matrix.mtx> [iterations] | --laplace <grid> [it] | "
-                        "--powerlaw <rows> [it]\n", argv[0]);
+                        "--powerlaw <rows> [it], then optionally --sell\n", argv[0]);
         return 2;
     }
     Csr A;
@@ -235,5 +243,21 @@ int main(int argc, char **argv) {
     print_record(name, "CSR5", rec, A.m, A.n, nnz, y.data(), y_ref.data(), absum.data(), bad,
                  peak);
     failures += (st != 0) + (bad != 0);
+    if (with_sell) {
+        printf("**************\n     SELL     \n**************\n");
+        pava_init_vectors(A.m, A.n, nullptr, y.data(), nullptr);
+        pava_run_record srec;
+        const int sst = pava_conduct(PAVA_FORMAT_SELL, &csr, x.data(), y.data(), cname.data(),
+                                     iters, &opts, &srec);
+        if (sst == PAVA_E_UNSUPPORTED_PARAMS) {  // the slices would pad too much: not a failure
+            printf("SELL refuses the matrix: %s\n", pava_last_error());
+        } else {
+            const int sbad = check_results(A.m, y.data(), y_ref.data());
+            printf("SELL status %d, rows off by more than 1%%: %d\n", sst, sbad);
+            print_record(name, "SELL", srec, A.m, A.n, nnz, y.data(), y_ref.data(),
+                         absum.data(), sbad, peak);
+            failures += (sst != 0) + (sbad != 0);
+        }
+    }
     return failures ? 1 : 0;
 }

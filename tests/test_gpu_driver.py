@@ -49,3 +49,23 @@ def test_driver_mtx_and_small_cvr_guard(cuda, tmp_path):
     lines = PERF.findall(out)
     assert lines[0][1] == "CVR" and float(lines[0][3]) == -1.0   # skipped, as in main.cpp
     assert lines[1][1] == "CSR5" and float(lines[1][4]) > 0
+
+
+def test_driver_sell_section(cuda, tmp_path):
+    """--sell adds a SELL section: on the Laplacian a Performance line and a record passing the
+    same checks; on a power-law matrix one line saying why the form refuses it."""
+    rc, out = _run("--laplace", "512", "50", "--sell")
+    assert rc == 0, out
+    assert "SELL status 0, rows off by more than 1%: 0" in out
+    assert re.search(r"^ Performance laplace_512 SELL (\d+) ([0-9.]+) ([0-9.]+) $", out, re.M), out
+    recs = [json.loads(l) for l in out.splitlines() if l.startswith('{"record": "pava_bench"')]
+    assert [r["section"] for r in recs] == ["CVR", "CSR5", "SELL"]
+    assert recs[2]["max_rel_err"] <= 1e-12 and recs[2]["rows_off_1pct"] == 0
+    from pava_b200 import matrices as M
+    A = M.powerlaw(8000, mean=8.0, seed=11)
+    assert not M.sell_accepts(A)
+    path = os.path.join(tmp_path, "pl.mtx")
+    M.write_mtx(path, A)
+    rc, out = _run(path, "5", "--sell")
+    assert rc == 0, out
+    assert "SELL refuses the matrix: SELL: padding" in out
