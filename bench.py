@@ -654,6 +654,9 @@ def precision_form(torch, stream):
                     "speedup_fp32c_over_fp64": round(out["fp64"]["ms"] / out["fp32c"]["ms"], 3),
                     "speedup_fp32c_over_fp64_d16": round(out["fp64_d16"]["ms"]
                                                          / out["fp32c"]["ms"], 3),
+                    # against the reference's own format (CSR5, FP64, 32-bit columns)
+                    "speedup_fp32c_over_fp64_csr5": round(
+                        out["sweep_ms"]["fp64 csr5_sigma32"] / out["fp32c"]["ms"], 3),
                     "max_rel_err_vs_fp64": float(rel.max()),
                     "mean_rel_err_vs_fp64": float(rel.mean()), "error_bound": 1e-9})
         return out
