@@ -26,6 +26,16 @@ int pava_probe_floor(int mode, const double *vals, const int *cols, const double
                      int threads, double *out, void *stream);
 long long pava_probe_floor_out_len(int blocks_per_sm, int threads);
 
+/* The gathers of mode 1 (x[hash(i, seed) mod n], the first nnz rounded down to 32 elements)
+ * fetched by the TMA engine: x (16-byte aligned, n even) viewed as n / 2 rows of 16 bytes under
+ * a 2-D tensor map, cp.async.bulk.tensor tile::gather4 into shared memory, bounded mbarrier
+ * waits (a wait that gives up counts in *wait_fail, device memory).  blocks_per_sm x SMs blocks
+ * of 256 threads; `out` receives one double per warp (pava_probe_floor_out_len(blocks_per_sm,
+ * 256) entries), summing to mode 1's total over the same elements.  Returns 0, -10 or -12. */
+int pava_probe_gather_tma(const double *x, long long nnz, int n, unsigned long long seed,
+                          int blocks_per_sm, double *out, unsigned long long *wait_fail,
+                          void *stream);
+
 #ifdef __cplusplus
 }
 #endif

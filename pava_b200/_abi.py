@@ -183,6 +183,8 @@ PROBE_SYMBOLS = [
     ("pava_probe_floor", c_int, [c_int, c_void_p, c_void_p, c_void_p, c_ll, c_int, c_u64, c_int,
                                  c_int, c_void_p, c_void_p]),
     ("pava_probe_floor_out_len", c_ll, [c_int, c_int]),
+    ("pava_probe_gather_tma", c_int, [c_void_p, c_ll, c_int, c_u64, c_int, c_void_p, c_void_p,
+                                      c_void_p]),
 ]
 _PROBE = None
 

@@ -107,7 +107,8 @@ def build_probe(force: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     out = os.path.join(LIBDIR, "libpava_probe.so")
     src = os.path.join(CSRC, "k_probe.cu")
-    deps = [src, os.path.join(CSRC, "pava_common.cuh"), os.path.join(ROOT, "include", "pava_probe.h")]
+    deps = [src, os.path.join(CSRC, "pava_common.cuh"), os.path.join(CSRC, "k_bulk.cuh"),
+            os.path.join(ROOT, "include", "pava_probe.h")]
     if not force and not _stale(out, deps):
         return out
     _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",

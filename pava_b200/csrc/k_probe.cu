@@ -11,16 +11,25 @@
 //   GATHERS  x at columns drawn by a hash, no streams:  sum x[h(i) mod n]   one 8-byte gather
 //   COLGATH  the column stream and x at those columns:  sum x[c]            4 B + one gather
 //   DOT      values, columns and x at the columns:      sum v * x[c]        12 B + one gather
+//   TMAGATH  GATHERS' x values fetched by the TMA engine instead of the load units: x viewed as
+//            n / 2 rows of 16 bytes under a 2-D tensor map, lanes 0..7 of a warp each issue one
+//            cp.async.bulk.tensor tile::gather4 (four rows, box one row high) per 32 elements
+//            into shared memory, completion on an mbarrier (bounded waits), lane l then reads
+//            its value there -- the other gather path of sm_100, measured beside the L1 one
 //
 // No counterpart in the reference: a measurement aid only (pava_probe.h).
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "../../include/pava_probe.h"
+#include "k_bulk.cuh"
 #include "pava_common.cuh"
 
 namespace pava {
 namespace {
 
-enum { STREAMS = 0, GATHERS = 1, COLGATH = 2, DOT = 3 };
+enum { STREAMS = 0, GATHERS = 1, COLGATH = 2, DOT = 3, TMAGATH = 4 };
 
 __device__ __forceinline__ unsigned hash_col(unsigned long long i, unsigned long long seed,
                                              unsigned n) {
@@ -97,8 +106,110 @@ __global__ void floor_kernel(const double *__restrict__ vals, const int *__restr
     if ((threadIdx.x & 31) == 0) out[tid >> 5] = acc;
 }
 
+// TMAGATH: 8 warps per CTA; per warp and step 32 elements, eight gather4 pieces of 64 bytes
+// (each at a 128-byte boundary) in one of two 1 KB slots, one mbarrier per slot.
+constexpr int TMA_WARPS = 8;
+__global__ void __launch_bounds__(TMA_WARPS * 32)
+tma_gather_kernel(const __grid_constant__ CUtensorMap tmap, long long nnz, int n,
+                  unsigned long long seed, double *__restrict__ out,
+                  unsigned long long *__restrict__ wait_fail) {
+    __shared__ __align__(128) unsigned char slots[TMA_WARPS][2][1024];
+    __shared__ __align__(8) unsigned long long bars[TMA_WARPS][2];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned bar0 = (unsigned)__cvta_generic_to_shared(&bars[w][0]);
+    if (lane == 0) {
+        mbar_init(bar0);
+        mbar_init(bar0 + 8);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    const long long nwarps = (long long)gridDim.x * TMA_WARPS;
+    const long long wid = (long long)blockIdx.x * TMA_WARPS + w;
+    const long long steps = nnz / 32;  // whole steps of 32 elements
+    auto issue = [&](long long step, int b) {
+        if (lane < 8) {
+            const unsigned long long i0 = (unsigned long long)step * 32 + lane * 4;
+            int rows[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) rows[j] = (int)(hash_col(i0 + j, seed, n) >> 1);
+            const unsigned bar = bar0 + 8 * b;
+            if (lane == 0) mbar_expect_tx(bar, 8 * 64);
+            __syncwarp(0xffu);
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(&slots[w][b][lane * 128]);
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::"
+                "complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+                ::"r"(dst), "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(0), "r"(rows[0]),
+                  "r"(rows[1]), "r"(rows[2]), "r"(rows[3]), "r"(bar)
+                : "memory");
+        }
+    };
+    double acc = 0.0;
+    unsigned phase = 0;
+    int b = 0, pending = 0;
+    long long st = wid;
+    if (st < steps) { issue(st, 0); ++pending; }
+    if (st + nwarps < steps) { issue(st + nwarps, 1); ++pending; }
+    bool ok = true;
+    for (; st < steps; st += nwarps) {
+        if (!mbar_wait(bar0 + 8 * b, (phase >> b) & 1u)) {
+            if (lane == 0) atomicAdd(wait_fail, 1ull);
+            ok = false;
+            break;
+        }
+        phase ^= 1u << b;
+        --pending;
+        const unsigned c = hash_col((unsigned long long)st * 32 + lane, seed, n);
+        const double *piece = reinterpret_cast<const double *>(&slots[w][b][(lane >> 2) * 128]);
+        acc += piece[(lane & 3) * 2 + (c & 1)];
+        __syncwarp();
+        if (lane == 0) proxy_fence();
+        __syncwarp();
+        if (st + 2 * nwarps < steps) { issue(st + 2 * nwarps, b); ++pending; }
+        b ^= 1;
+    }
+    for (; !ok && pending > 0; --pending) {  // after a wait gave up: let copies in flight land
+        mbar_wait(bar0 + 8 * b, (phase >> b) & 1u);
+        phase ^= 1u << b;
+        b ^= 1;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) out[wid] = acc;
+}
+
 }  // namespace
 }  // namespace pava
+
+extern "C" int pava_probe_gather_tma(const double *x, long long nnz, int n,
+                                     unsigned long long seed, int blocks_per_sm, double *out,
+                                     unsigned long long *wait_fail, void *stream) {
+    using namespace pava;
+    if (!x || ((uintptr_t)x & 15) || n <= 0 || (n & 1) || nnz < 0 || blocks_per_sm <= 0 ||
+        !out || !wait_fail)
+        return -10;
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+        return -12;
+    auto encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    CUtensorMap tmap;
+    const cuuint64_t dims[2] = {2, (cuuint64_t)n / 2};  // x as n / 2 rows of two doubles
+    const cuuint64_t strides[1] = {16};
+    const cuuint32_t box[2] = {2, 1};  // one row high, as tile::gather4 wants
+    const cuuint32_t estr[2] = {1, 1};
+    if (encode(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)x, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return -12;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return -12;
+    tma_gather_kernel<<<(unsigned)(sms * blocks_per_sm), TMA_WARPS * 32, 0,
+                        (cudaStream_t)stream>>>(tmap, nnz, n, seed, out, wait_fail);
+    return cudaGetLastError() == cudaSuccess ? 0 : -12;
+}
 
 extern "C" int pava_probe_floor(int mode, const double *vals, const int *cols, const double *x,
                                 long long nnz, int n, unsigned long long seed,

@@ -18,8 +18,9 @@ SpMM) kernel (CUDA events) unless --quiet.
 
 ``--floor`` runs the floor kernels of include/pava_probe.h on the matrix's CSR arrays instead
 (streams only, gathers at hashed columns only, column stream + gathers, values + columns +
-gathers), each over a sweep of blocks per SM, and prints the fastest launch shape of each:
-the two costs an SpMV on this matrix is made of, measured apart.
+gathers; mode 4: the gathers of mode 1 fetched by the TMA engine with tile::gather4, its total
+checked against mode 1's), each over a sweep of blocks per SM, and prints the fastest launch
+shape of each: the two costs an SpMV on this matrix is made of, measured apart.
 """
 from __future__ import annotations
 
@@ -75,7 +76,8 @@ def main():
                    help="right-hand sides: k > 1 times pava_spmm on X (n x k, row-major); "
                         "CSR variants only")
     p.add_argument("--floor-modes", default="0,1,2,3",
-                   help="floor kernels to run (0 streams, 1 gathers, 2 cols+gathers, 3 dot)")
+                   help="floor kernels to run (0 streams, 1 gathers, 2 cols+gathers, 3 dot, "
+                        "4 the gathers of 1 by TMA tile::gather4)")
     p.add_argument("--floor-bps", default="2,4,8,16", help="blocks per SM to sweep")
     p.add_argument("--floor", action="store_true",
                    help="time the floor kernels (pava_probe.h) on the matrix instead")
@@ -154,7 +156,7 @@ def main():
 
 
 FLOOR_MODES = {0: ("streams", 12), 1: ("gathers", 0), 2: ("cols+gathers", 4),
-               3: ("vals+cols+gathers", 12)}
+               3: ("vals+cols+gathers", 12), 4: ("gathers by TMA gather4", 0)}
 
 
 def run_floors(torch, A, x_host, reps, quiet, modes=(0, 1, 2, 3), bps_list=(2, 4, 8, 16)):
@@ -166,32 +168,50 @@ def run_floors(torch, A, x_host, reps, quiet, modes=(0, 1, 2, 3), bps_list=(2, 4
     v = torch.from_numpy(A.v).cuda()
     x = torch.from_numpy(x_host).cuda()
     s = torch.cuda.current_stream().cuda_stream
+    fail = torch.zeros(1, dtype=torch.int64, device="cuda")
     for mode in modes:
         name, bpe = FLOOR_MODES[mode]
+        nnz = A.nnz if mode != 4 else A.nnz // 32 * 32  # whole warp steps for the TMA path
         best = None
         for bps in bps_list:
             out = torch.empty(P.pava_probe_floor_out_len(bps, 256), dtype=torch.float64,
                               device="cuda")
-            args = (mode, v.data_ptr(), ci.data_ptr(), x.data_ptr(), A.nnz, A.n, 1, bps, 256,
-                    out.data_ptr(), s)
+            if mode == 4:
+                def launch(bps=bps, out=out):
+                    return P.pava_probe_gather_tma(x.data_ptr(), nnz, A.n, 1, bps,
+                                                   out.data_ptr(), fail.data_ptr(), s)
+            else:
+                def launch(bps=bps, out=out, mode=mode):
+                    return P.pava_probe_floor(mode, v.data_ptr(), ci.data_ptr(), x.data_ptr(),
+                                              A.nnz, A.n, 1, bps, 256, out.data_ptr(), s)
             for _ in range(2):
-                if P.pava_probe_floor(*args) != 0:
-                    raise RuntimeError(f"pava_probe_floor mode {mode} failed")
+                if launch() != 0:
+                    raise RuntimeError(f"floor mode {mode} failed")
             ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                   for _ in range(reps)]
             for e0, e1 in ev:
                 e0.record()
-                P.pava_probe_floor(*args)
+                launch()
                 e1.record()
             torch.cuda.synchronize()
             t = sorted(e0.elapsed_time(e1) for e0, e1 in ev)[len(ev) // 2]
             if best is None or t < best[0]:
-                best = (t, bps)
-        t, bps = best
+                best = (t, bps, float(out.sum()))
+        t, bps, total = best
         line = {"floor": name, "mode": mode, "matrix_nnz": A.nnz, "n": A.n, "ms": t,
                 "blocks_per_sm": bps, "threads": 256,
                 "stream_GBps": bpe * A.nnz / (t * 1e-3) / 1e9 if bpe else None,
-                "gathers_per_s": A.nnz / (t * 1e-3) if mode else None}
+                "gathers_per_s": nnz / (t * 1e-3) if mode else None}
+        if mode == 4:  # the same gathers as mode 1 over the same elements: the same total
+            ref = torch.empty(P.pava_probe_floor_out_len(2, 256), dtype=torch.float64,
+                              device="cuda")
+            if P.pava_probe_floor(1, v.data_ptr(), ci.data_ptr(), x.data_ptr(), nnz, A.n, 1, 2,
+                                  256, ref.data_ptr(), s) != 0:
+                raise RuntimeError("floor mode 1 failed")
+            r = float(ref.sum())
+            line.update({"total": total, "mode1_total": r,
+                         "totals_agree": abs(total - r) <= 1e-9 * max(1.0, abs(r)),
+                         "wait_failures": int(fail.item())})
         if not quiet:
             print(json.dumps(line), flush=True)
 
